@@ -1,0 +1,412 @@
+"""Benchmark: ray-steps/s of the B200 tracer on the 512^3 turbulent box with
+1e7 rays, with the all-FP64 port and the error against it, end-to-end
+throughput through the public API, the trace kernel's roofline and the CPU
+baseline. Prints one JSON line (rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sloth|reference]
+
+One bench step = one trace of every ray of the workload (Morton pre-pass +
+persistent tracer). Multi-GPU runs shard nothing across ranks: each rank
+traces its own seeded 1e7-ray beam through its own copy of the grid (weak
+scaling; rays are independent, there is no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ray-steps/s, 512³ turb box 1e7 rays, ≤1e-6 rel err vs all-FP64 kernel; p99 latency"
+UNIT = "ray-steps/s"
+BYTES_PER_RAY_STEP = 512          # 4 RK4 stages x 8 corners x 16-byte float4 voxels
+L = 5e-3
+LWL = 532e-9
+TE, ZION = 20.0, 1.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["sloth", "reference"], default="sloth")
+    ap.add_argument("--n", type=int, default=512, help="grid points per axis")
+    ap.add_argument("--rays", type=float, default=1e7)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per trace launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "trace_kernel_kolmogorov512_1e7.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_workload(n, nrays, seed, device):
+    import torch
+    from sloth_b200 import workloads
+    ne = workloads.kolmogorov_box(n, L=L, mean=1e25, rms=0.2, seed=seed, device=device)
+    rays = workloads.gaussian_beam(nrays, waist=1.5e-3, L=L, seed=seed + 1, device=device)
+    torch.cuda.synchronize()
+    return ne, rays
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the oracle's C restatement of the reference on host cores
+# ---------------------------------------------------------------------------
+def cpu_oracle_rate(ne_host, rays_host, spacing, omega, dtau, n_steps, seconds, threads=0):
+    """Time the FP64 C restatement on a bounded ray sample; returns
+    (ray-steps/s, sample description, threads, total_steps)."""
+    from oracle import oracle_c
+    from oracle import ref_restated as rr
+    grid = rr.Grid(ne_host.astype(np.float64), (-L / 2,) * 3, spacing, omega, Te=TE, Z=ZION)
+    thr = threads or oracle_c.threads()
+    probe = min(rays_host.shape[1], 64 * thr)
+    kw = dict(dtau=dtau, first_save=n_steps, save_every=1, n_saves=1, project=True, plane=L / 2,
+              inv_brems=True, threads=thr, want_state=False)
+    t0 = time.perf_counter()
+    r = oracle_c.trace_rays(grid, rays_host[:, :probe], **kw)
+    dt = time.perf_counter() - t0
+    rate = r["total_steps"] / dt
+    m = int(min(rays_host.shape[1], max(probe, rate * seconds / max(r["total_steps"] / probe, 1))))
+    t0 = time.perf_counter()
+    r = oracle_c.trace_rays(grid, rays_host[:, :m], **kw)
+    dt = time.perf_counter() - t0
+    return r["total_steps"] / dt, f"first {m} rays of the 1e7-ray beam, all steps", thr, r["total_steps"]
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+    from sloth_b200 import runtime, workloads
+    from sloth_b200.core import physics
+    n = args.n
+    h = L / (n - 1)
+    ne = workloads.kolmogorov_box(n, L=L, mean=1e25, rms=0.2, seed=args.seed, device="cpu").numpy()
+    rays = workloads.gaussian_beam(int(args.rays), waist=1.5e-3, L=L, seed=args.seed + 1).double().numpy()
+    omega = physics.omega_of(LWL)
+    sched = runtime.schedule_times([math.sqrt(8.0) * L], (h, h, h))
+    from oracle import oracle_c
+    from oracle import ref_restated as rr
+    grid = rr.Grid(ne.astype(np.float64), (-L / 2,) * 3, (h, h, h), omega, Te=TE, Z=ZION)
+    thr = oracle_c.threads()
+    per_step = max(64 * thr, 2000)
+    kw = dict(dtau=sched.dtau, first_save=sched.first_save, save_every=1, n_saves=1, project=True, plane=L / 2,
+              inv_brems=True, threads=thr, want_state=False)
+    times, steps = [], []
+    for i in range(args.warmup + args.steps):
+        lo = (i * per_step) % rays.shape[1]
+        sub = rays[:, lo:lo + per_step]
+        t0 = time.perf_counter()
+        r = oracle_c.trace_rays(grid, sub, **kw)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+            steps.append(r["total_steps"])
+    value = float(np.sum(steps) / np.sum(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{n}^3 Kolmogorov turbulent box (mean 1e19 cm^-3, 20% RMS), 1e7-ray 3 mm "
+                               f"Gaussian beam, 532 nm, Te=20 eV, Z=1; each step a {per_step}-ray sample",
+                   "note": "the reference (JAX/diffrax) cannot be installed on this image; its CPU path is "
+                           "stood in for by the oracle's FP64 C restatement (fixed-step RK4)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port",
+                         "sample": f"{per_step} rays per step, {args.steps} steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def run_sloth(args):
+    import torch
+    from sloth_b200 import _capi, runtime
+    from sloth_b200.core import physics
+    from sloth_b200.core.propagator import solve
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    n, nrays = args.n, int(args.rays)
+    h = L / (n - 1)
+    omega = physics.omega_of(LWL)
+    seed = args.seed + 1000 * rank
+    ne, rays = make_workload(n, nrays, seed, dev)
+    grid = runtime.pack_grid(ne, (-L / 2,) * 3, (h, h, h), omega, precision="f32")
+    sched = runtime.schedule_times([math.sqrt(8.0) * L], (h, h, h))
+    stream = torch.cuda.current_stream()
+    outs = {}
+    ws = None
+
+    def step(ev=None):
+        return runtime.trace(grid, rays, sched, project=True, plane=L / 2, inv_brems=True, Te=TE, Z=ZION,
+                             want_status=True, want_steps=False, outputs=outs, events=ev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for a, b in kev:
+        a.record()
+        b.record()
+    torch.cuda.synchronize()
+    launches0 = _capi.launch_count()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier()
+        for i in range(args.steps):
+            evs[i][0].record(stream)
+            step(kev[i])
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    launches = _capi.launch_count() - launches0
+    per_step_ms = [a.elapsed_time(b) for a, b in evs]
+    kernel_ms = [a.elapsed_time(b) for a, b in kev]
+    total_ms = evs[0][0].elapsed_time(evs[-1][1])
+    ray_steps = int(outs["total_steps"][0])
+    if dist is not None:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t[0])
+        s = torch.tensor([ray_steps], device=dev, dtype=torch.float64)
+        dist.all_reduce(s)
+        all_ray_steps = float(s[0])
+    else:
+        all_ray_steps = float(ray_steps)
+    value = all_ray_steps * args.steps / (total_ms / 1e3)
+    f32_out = {k: v.clone() for k, v in outs.items()}
+
+    # ---- all-FP64 port of the same kernel on the same workload -------------
+    fp64 = None
+    acc = None
+    if not args.no_fp64:
+        g64 = runtime.pack_grid(ne, (-L / 2,) * 3, (h, h, h), omega, precision="f64")
+        r64 = rays.double()
+        o64 = {}
+        for _ in range(1):
+            runtime.trace(g64, r64, sched, project=True, plane=L / 2, inv_brems=True, Te=TE, Z=ZION,
+                          want_steps=False, outputs=o64)
+        torch.cuda.synchronize()
+        k2 = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        k2[0].record()
+        k2[1].record()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 2
+        ktimes = []
+        e0.record(stream)
+        for _ in range(reps):
+            runtime.trace(g64, r64, sched, project=True, plane=L / 2, inv_brems=True, Te=TE, Z=ZION,
+                          want_steps=False, outputs=o64, events=k2)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ktimes.append(k2[0].elapsed_time(k2[1]))
+        ms64 = e0.elapsed_time(e1) / reps
+        rs64 = int(o64["total_steps"][0])
+        fp64 = {"value": rs64 / (ms64 / 1e3), "ms_per_step": ms64, "kernel_ms": float(np.mean(ktimes)),
+                "ray_steps": rs64}
+        # accuracy of the FP32 split kernel against the FP64 port (all rays)
+        j32, j64 = f32_out["jones"][-1].double(), o64["jones"][-1]
+        ok = (f32_out["status"] != 2) & (o64["status"] != 2)
+        dpos = torch.maximum((j32[0] - j64[0]).abs(), (j32[2] - j64[2]).abs())[ok] / L
+        dang = torch.maximum((j32[1] - j64[1]).abs(), (j32[3] - j64[3]).abs())[ok]
+        ph64 = o64["phase"][-1][ok]
+        dph = (f32_out["phase"][-1][ok] - ph64).abs()
+        damp = (f32_out["amp"][-1].double() - o64["amp"][-1])[ok].abs()
+
+        def q(t, p):
+            t = t.float() if t.numel() < 2 ** 24 else t[:: max(1, t.numel() // 2 ** 23)].float()
+            return float(torch.quantile(t, p))
+        acc = {"position_rel_L_max": float(dpos.max()), "position_rel_L_p99": q(dpos, 0.99),
+               "angle_abs_max_rad": float(dang.max()), "angle_abs_p99_rad": q(dang, 0.99),
+               "phase_abs_max_rad": float(dph.max()), "phase_max_abs_rad": float(ph64.abs().max()),
+               "phase_rel_max": float(dph.max() / ph64.abs().max()),
+               "amp_abs_max": float(damp.max()), "rays_compared": int(ok.sum()),
+               "status_mismatch": int((f32_out["status"] != o64["status"]).sum())}
+        del g64, r64, o64
+
+    # ---- end to end through the public API (host buffers) -------------------
+    e2e = None
+    if not args.no_e2e:
+        import types
+        ne_host = ne.cpu().pin_memory()
+        rays_host = rays.cpu().pin_memory()
+        c1 = np.linspace(-L / 2, L / 2, n).astype(np.float32)
+        dom = types.SimpleNamespace(ne=ne_host, x=c1, y=c1, z=c1, probing_direction='z',
+                                    lengths=np.array([L] * 3, np.float32), dims=np.array([n] * 3),
+                                    Np_total=None, inv_brems=True, Te=np.float32(TE), Z=np.float32(ZION),
+                                    region_count=1, ray_batch_count=1)
+        res = None
+        for _ in range(1):
+            res = solve(rays_host, dom, L, lwl=LWL, verbose=False, detector_plane=L / 2, return_extras=True)
+        torch.cuda.synchronize()
+        reps = max(2, min(args.steps, 3))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            res = solve(rays_host, dom, L, lwl=LWL, verbose=False, detector_plane=L / 2, return_extras=True)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / reps
+        rf, amp, _, ex = res
+        d2h = rf.nbytes + amp.nbytes + ex["phase"].nbytes + ex["status"].nbytes + ex["steps"].nbytes
+        h2d = ne_host.numel() * ne_host.element_size() + rays_host.numel() * rays_host.element_size()
+        e2e = {"value": ex["total_steps"] / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3,
+               "path": "sloth_b200.core.propagator.solve (pinned host ne and rays, numpy outputs)"}
+
+    # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, sample, thr, _ = cpu_oracle_rate(ne.cpu().numpy(), rays.double().cpu().numpy(), (h, h, h), omega,
+                                               sched.dtau, sched.first_save, args.cpu_seconds)
+        cpu = {"value": rate, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        kms = float(np.mean(kernel_ms))
+        achieved = ray_steps * BYTES_PER_RAY_STEP / (kms / 1e3) / 1e9
+        traffic = committed_traffic()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{n}^3 Kolmogorov turbulent box (mean 1e19 cm^-3, 20% RMS, k^-11/3), "
+                                   f"{nrays:.0e} rays, 3 mm Gaussian beam along +z, 532 nm, Te=20 eV, Z=1, "
+                                   "fixed-step RK4 ds=h/2, detector plane z=+2.5 mm",
+                       "l2": "inputs larger than L2 (2.1 GB packed grid, 240 MB rays)",
+                       "precision": "FP32 state with compensated sums, FP64 phase, Kahan FP32 optical depth",
+                       "seed": args.seed, "ray_steps_per_trace": ray_steps},
+            "latency_ms": {"p50": float(np.percentile(per_step_ms, 50)), "p99": float(np.percentile(per_step_ms, 99)),
+                           "what": "one 1e7-ray trace per request"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_kind": f"{peak_kind} HBM copy bandwidth",
+                         "kernel": "trace_kernel<PolF32>", "kernel_ms": kms,
+                         "bytes_per_ray_step": BYTES_PER_RAY_STEP},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "fp64_port": fp64,
+            "fp32_vs_fp64": acc,
+        }
+        if fp64:
+            line["fp64_port"]["speedup_of_fp32"] = value / world / fp64["value"]
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_sloth(args)
+
+
+if __name__ == "__main__":
+    main()

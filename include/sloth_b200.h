@@ -1,0 +1,159 @@
+/*
+ * sloth_b200.h — C ABI of the B200 (sm_100a) ray-propagation library.
+ *
+ * The library replaces the hot path of SLOTH's JAX propagator: the grid-level
+ * precompute, the trilinear interpolator, the RHS and the vmapped diffrax solve,
+ * and the Jones-vector projection at the end of a trace. Every entry point:
+ *   - returns SLOTH_OK (0) or a negative SLOTH_ERR_* code (never throws, never
+ *     exits, never aborts); sloth_strerror() turns a code into text;
+ *   - takes caller-owned DEVICE buffers as plain pointers (e.g. torch
+ *     tensor.data_ptr()); nothing here allocates device memory except the
+ *     request server, which owns one arena sized by its HBM budget;
+ *   - launches asynchronously on the caller's CUDA stream (`stream` is a
+ *     cudaStream_t passed as void*; NULL = the legacy default stream).
+ *
+ * Units: positions in metres, velocities in m/s, densities in m^-3, time as
+ * path length tau = c*t in metres. Ray arrays are row-major (6, N):
+ * rows x, y, z, vx, vy, vz, exactly the layout of the reference's Beam.s0.
+ */
+#ifndef SLOTH_B200_H
+#define SLOTH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SLOTH_ABI_VERSION 1
+
+/* ---- return codes ------------------------------------------------------ */
+#define SLOTH_OK                        0
+#define SLOTH_ERR_INVALID_ARGUMENT     -1
+#define SLOTH_ERR_NULL_POINTER         -2
+#define SLOTH_ERR_MISALIGNED           -3
+#define SLOTH_ERR_WORKSPACE_TOO_SMALL  -4
+#define SLOTH_ERR_CUDA                 -5
+#define SLOTH_ERR_NO_DEVICE            -6
+#define SLOTH_ERR_TOO_LARGE            -7
+#define SLOTH_ERR_OUT_OF_MEMORY        -8
+#define SLOTH_ERR_NOT_FOUND            -9
+#define SLOTH_ERR_BUSY                -10
+#define SLOTH_ERR_UNSUPPORTED_DEVICE  -11
+
+/* ---- per-ray status written by the tracers ---------------------------- */
+#define SLOTH_RAY_EXITED          0  /* left the grid and can never re-enter   */
+#define SLOTH_RAY_INSIDE_AT_END   1  /* still inside the grid at the last save */
+#define SLOTH_RAY_NONFINITE       2  /* state became NaN/Inf; outputs are NaN  */
+
+/* Uniform grid: point i of axis a sits at origin[a] + i*spacing[a].
+ * Voxel (i, j, k) is element (i*n[1] + j)*n[2] + k (C order, z fastest),
+ * which is numpy's layout of an (nx, ny, nz) array. */
+typedef struct SlothGridDesc {
+    int32_t n[3];        /* points per axis, each >= 2                        */
+    int32_t reserved;    /* must be 0                                         */
+    double  origin[3];   /* coordinate of point 0 per axis (m)                */
+    double  spacing[3];  /* uniform spacing per axis (m), > 0                 */
+} SlothGridDesc;
+
+/* Fixed-step RK4 schedule and physics of one trace.
+ * All steps have the same length dtau (tau = c*t, metres). Save j (0-based)
+ * is taken after step first_save + j*save_every; the trace ends at the last
+ * save. Rays that have left the grid for good are advanced to later saves by
+ * exact straight-line drift (the RHS is zero outside the grid). */
+typedef struct SlothTraceParams {
+    double  omega;            /* laser angular frequency (rad/s)                    */
+    double  dtau;             /* step length in c*t (m), > 0                        */
+    int32_t first_save;       /* step index of save 0, >= 0                         */
+    int32_t save_every;       /* steps between saves, >= 1 when n_saves > 1         */
+    int32_t n_saves;          /* number of saves, 1 .. SLOTH_MAX_SAVES              */
+    int32_t probing_axis;     /* 0 = x, 1 = y, 2 = z                                */
+    int32_t project_to_plane; /* 0: Jones vector at the ray's current position
+                                 (reference keep_current_plane=True); 1: the ray's
+                                 straight line back-projected to `plane`
+                                 (keep_current_plane=False, ne_extent = plane)      */
+    int32_t inv_brems;        /* 1: accumulate inverse-bremsstrahlung optical depth */
+    double  plane;            /* detector plane along probing_axis (m)              */
+    double  kappa_q2;         /* kappa/c per (ne/nc)^2 with the Coulomb log factored
+                                 out (1/m): 3.1e-5*Z*(nc_cc/omega)^2*Te^-1.5        */
+    double  coulomb_log_w;    /* ln(v_the/(omega*b_min)): Coulomb log for ne < nc   */
+    double  ope_ratio2;       /* (omega_pe/omega)^2 per unit ne/nc (NRL constants)  */
+} SlothTraceParams;
+
+#define SLOTH_MAX_SAVES 4096
+
+/* Output buffers of a trace; element type follows the entry point
+ * (float for *_f32, double for *_f64) unless stated. Arrays with a save axis
+ * are [n_saves][rows][N] row-major. NULL skips an optional output. */
+typedef struct SlothTraceOutputs {
+    void*     jones;        /* [S][4][N] required: rows (pos1, angle1, pos2, angle2)
+                               in the reference's ray_to_Jonesvector order          */
+    void*     state;        /* [S][6][N] optional: x,y,z (m), vx,vy,vz (m/s)        */
+    double*   phase;        /* [S][N] optional, always double: optical phase
+                               integral of omega*(n-1) dt (rad)                     */
+    void*     amp;          /* [S][N] optional: exp(-tau_ib); needs inv_brems       */
+    uint8_t*  status;       /* [N] optional: SLOTH_RAY_*                            */
+    int32_t*  steps;        /* [N] optional: RK4 steps taken before exit / end      */
+    unsigned long long* total_steps; /* [1] optional device counter: sum of steps,
+                               zeroed by the entry point before the launch          */
+    void*     trace_event_begin; /* optional cudaEvent_t recorded on `stream` right
+                               before the tracer kernel (after the sort pre-pass)   */
+    void*     trace_event_end;   /* optional cudaEvent_t recorded right after it     */
+} SlothTraceOutputs;
+
+/* ---- library info ------------------------------------------------------ */
+const char* sloth_strerror(int code);
+int  sloth_abi_version(void);
+/* Device properties of the current CUDA device. */
+int  sloth_device_info(int* sm_count, int* cc_major, int* cc_minor);
+/* Number of kernels this library has launched in this process. */
+unsigned long long sloth_launch_count(void);
+
+/* ---- K1: grid pack ------------------------------------------------------
+ * Replaces precompute_gradients (src/core/propagator.py:39-93) and the
+ * reference's per-grid kappa precompute (:116-164, folded into the tracer).
+ * Writes one voxel-packed (q, dq/du, dq/dv, dq/dw) per grid point, where
+ * q = ne * ne_scale (ne_scale = 1/nc) and d/du is the derivative per grid
+ * cell: central differences inside, one-sided at the faces (jnp.gradient
+ * semantics, :90-92). ne is float32 (ne_is_f64 = 0) or float64, C order.
+ * grid_out must be 16-byte aligned (f32: float4) / 16-byte aligned (f64:
+ * 2 x double2 per voxel). */
+size_t sloth_grid_bytes(const SlothGridDesc* g, int real_bytes /* 4 or 8 */);
+int sloth_grid_pack_f32(const SlothGridDesc* g, const void* ne, int ne_is_f64,
+                        double ne_scale, void* grid_out, void* stream);
+int sloth_grid_pack_f64(const SlothGridDesc* g, const void* ne, int ne_is_f64,
+                        double ne_scale, void* grid_out, void* stream);
+
+/* ---- K0: trilinear sample -----------------------------------------------
+ * Replaces RegularGridInterpolator (src/core/interpolator.py:15-105) on the
+ * packed grid: for each point (3, N) row-major in metres, writes the four
+ * interpolated channels (4, N): q and dq/du, dq/dv, dq/dw, with 0 outside
+ * the grid (fill_value = 0, :85-87, :102-104). */
+int sloth_sample_f32(const SlothGridDesc* g, const void* grid, const double* points,
+                     int64_t n, float* out, void* stream);
+int sloth_sample_f64(const SlothGridDesc* g, const void* grid, const double* points,
+                     int64_t n, double* out, void* stream);
+
+/* ---- K2/K3: tracers ------------------------------------------------------
+ * Replace the vmapped diffrax solve of dsdt (src/core/propagator.py:723-793,
+ * :1159-1198) and the Jones-vector projection of its result
+ * (src/shared/propagation.py:4-90, propagator.py:316-327, :1210-1218).
+ * _f32: FP32 state with compensated (Neumaier) position and velocity sums,
+ * FP32 float4 grid, FP64 phase accumulator, Kahan FP32 optical depth.
+ * _f64: the same kernel with every quantity in FP64 and a double grid.
+ * rays: (6, N) row-major, float (f32) or double (f64).
+ * workspace: device scratch of at least sloth_trace_workspace_bytes(N) bytes,
+ * 256-byte aligned; its contents need not be initialised. */
+size_t sloth_trace_workspace_bytes(int64_t n_rays);
+int sloth_trace_f32(const SlothGridDesc* g, const void* grid, const SlothTraceParams* p,
+                    const float* rays, int64_t n, const SlothTraceOutputs* out,
+                    void* workspace, size_t workspace_bytes, void* stream);
+int sloth_trace_f64(const SlothGridDesc* g, const void* grid, const SlothTraceParams* p,
+                    const double* rays, int64_t n, const SlothTraceOutputs* out,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SLOTH_B200_H */

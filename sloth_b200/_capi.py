@@ -1,0 +1,146 @@
+"""ctypes binding of ``libsloth_b200.so`` (declared in ``include/sloth_b200.h``).
+
+The library is the only compute path of this package: there is no CPU or
+PyTorch fallback. If the shared object is missing the import of this module
+raises ``SlothExtensionMissing``; if there is no usable sm_100 device, the
+compute entry points return ``SLOTH_ERR_NO_DEVICE`` /
+``SLOTH_ERR_UNSUPPORTED_DEVICE`` and ``check`` raises ``SlothError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import (POINTER, Structure, c_char_p, c_double, c_int, c_int32, c_int64,
+                    c_size_t, c_uint8, c_ulonglong, c_void_p)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libsloth_b200.so")
+
+SLOTH_OK = 0
+SLOTH_ERR_INVALID_ARGUMENT = -1
+SLOTH_ERR_NULL_POINTER = -2
+SLOTH_ERR_MISALIGNED = -3
+SLOTH_ERR_WORKSPACE_TOO_SMALL = -4
+SLOTH_ERR_CUDA = -5
+SLOTH_ERR_NO_DEVICE = -6
+SLOTH_ERR_TOO_LARGE = -7
+SLOTH_ERR_OUT_OF_MEMORY = -8
+SLOTH_ERR_NOT_FOUND = -9
+SLOTH_ERR_BUSY = -10
+SLOTH_ERR_UNSUPPORTED_DEVICE = -11
+
+SLOTH_RAY_EXITED = 0
+SLOTH_RAY_INSIDE_AT_END = 1
+SLOTH_RAY_NONFINITE = 2
+
+SLOTH_MAX_SAVES = 4096
+
+
+class SlothExtensionMissing(ImportError):
+    """The compiled CUDA library is not present (build it with ``make`` in csrc/)."""
+
+
+class SlothError(RuntimeError):
+    """A library entry point returned a negative status code."""
+
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        msg = strerror(code)
+        super().__init__(f"{what}: {msg} (code {code})" if what else f"{msg} (code {code})")
+
+
+class SlothGridDesc(Structure):
+    _fields_ = [("n", c_int32 * 3), ("reserved", c_int32),
+                ("origin", c_double * 3), ("spacing", c_double * 3)]
+
+
+class SlothTraceParams(Structure):
+    _fields_ = [("omega", c_double), ("dtau", c_double),
+                ("first_save", c_int32), ("save_every", c_int32), ("n_saves", c_int32),
+                ("probing_axis", c_int32), ("project_to_plane", c_int32), ("inv_brems", c_int32),
+                ("plane", c_double), ("kappa_q2", c_double), ("coulomb_log_w", c_double),
+                ("ope_ratio2", c_double)]
+
+
+class SlothTraceOutputs(Structure):
+    _fields_ = [("jones", c_void_p), ("state", c_void_p), ("phase", c_void_p),
+                ("amp", c_void_p), ("status", c_void_p), ("steps", c_void_p),
+                ("total_steps", c_void_p), ("trace_event_begin", c_void_p), ("trace_event_end", c_void_p)]
+
+
+# name -> (restype, argtypes); every symbol include/sloth_b200.h declares.
+_SIGNATURES = {
+    "sloth_strerror": (c_char_p, [c_int]),
+    "sloth_abi_version": (c_int, []),
+    "sloth_device_info": (c_int, [POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    "sloth_launch_count": (c_ulonglong, []),
+    "sloth_grid_bytes": (c_size_t, [POINTER(SlothGridDesc), c_int]),
+    "sloth_grid_pack_f32": (c_int, [POINTER(SlothGridDesc), c_void_p, c_int, c_double, c_void_p, c_void_p]),
+    "sloth_grid_pack_f64": (c_int, [POINTER(SlothGridDesc), c_void_p, c_int, c_double, c_void_p, c_void_p]),
+    "sloth_sample_f32": (c_int, [POINTER(SlothGridDesc), c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    "sloth_sample_f64": (c_int, [POINTER(SlothGridDesc), c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    "sloth_trace_workspace_bytes": (c_size_t, [c_int64]),
+    "sloth_trace_f32": (c_int, [POINTER(SlothGridDesc), c_void_p, POINTER(SlothTraceParams), c_void_p,
+                                c_int64, POINTER(SlothTraceOutputs), c_void_p, c_size_t, c_void_p]),
+    "sloth_trace_f64": (c_int, [POINTER(SlothGridDesc), c_void_p, POINTER(SlothTraceParams), c_void_p,
+                                c_int64, POINTER(SlothTraceOutputs), c_void_p, c_size_t, c_void_p]),
+}
+
+EXPORTED_SYMBOLS = tuple(_SIGNATURES)
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the library once; raise SlothExtensionMissing if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise SlothExtensionMissing(
+            f"{LIB_PATH} not found: build it with `make -C {os.path.join(_HERE, 'csrc')}` "
+            "(or __graft_entry__.build()); there is no fallback implementation")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def strerror(code: int) -> str:
+    try:
+        return load().sloth_strerror(int(code)).decode()
+    except SlothExtensionMissing:
+        return f"error {code}"
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != SLOTH_OK:
+        raise SlothError(rc, what)
+
+
+def launch_count() -> int:
+    return int(load().sloth_launch_count())
+
+
+def device_info():
+    sms, ma, mi = c_int(0), c_int(0), c_int(0)
+    check(load().sloth_device_info(ctypes.byref(sms), ctypes.byref(ma), ctypes.byref(mi)), "sloth_device_info")
+    return sms.value, ma.value, mi.value
+
+
+def grid_desc(n, origin, spacing) -> SlothGridDesc:
+    g = SlothGridDesc()
+    for a in range(3):
+        g.n[a] = int(n[a])
+        g.origin[a] = float(origin[a])
+        g.spacing[a] = float(spacing[a])
+    g.reserved = 0
+    return g
+
+
+def ptr(t) -> int:
+    """Device pointer of a torch tensor (or 0 for None)."""
+    return 0 if t is None else int(t.data_ptr())

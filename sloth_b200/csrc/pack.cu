@@ -1,0 +1,150 @@
+// K1 grid pack and K0 trilinear sample.
+//
+// K1 follows precompute_gradients (src/core/propagator.py:72-93): the driving
+// term is proportional to ne, and its gradient is taken with jnp.gradient
+// semantics along each axis (second-order central differences inside,
+// first-order one-sided differences on the two faces). Here the gradient is
+// kept per grid cell and normalised to the critical density, q = ne/nc; the
+// tracers fold the -c^2/2 and 1/h^2 factors into one per-axis constant.
+// All arithmetic is FP64; the FP32 grid rounds the final values once.
+#include "common.cuh"
+
+namespace sloth {
+
+template <class In>
+__device__ __forceinline__ double qat(const In* __restrict__ ne, size_t i, double scale) {
+    return (double)__ldg(ne + i) * scale;
+}
+
+template <class In, bool F64OUT>
+__global__ void __launch_bounds__(256) pack_kernel(const In* __restrict__ ne, void* __restrict__ out,
+                                                   GridGeo g, double scale, long long total) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < total; v += stride) {
+        const int k = (int)(v % g.n[2]);
+        const long long t = v / g.n[2];
+        const int j = (int)(t % g.n[1]);
+        const int i = (int)(t / g.n[1]);
+        const size_t vi = (size_t)v;
+        const double q = qat(ne, vi, scale);
+        double d0, d1, d2;
+        if (i == 0)               d0 = qat(ne, vi + g.sx, scale) - q;
+        else if (i == g.n[0] - 1) d0 = q - qat(ne, vi - g.sx, scale);
+        else                      d0 = 0.5 * (qat(ne, vi + g.sx, scale) - qat(ne, vi - g.sx, scale));
+        if (j == 0)               d1 = qat(ne, vi + g.sy, scale) - q;
+        else if (j == g.n[1] - 1) d1 = q - qat(ne, vi - g.sy, scale);
+        else                      d1 = 0.5 * (qat(ne, vi + g.sy, scale) - qat(ne, vi - g.sy, scale));
+        if (k == 0)               d2 = qat(ne, vi + 1, scale) - q;
+        else if (k == g.n[2] - 1) d2 = q - qat(ne, vi - 1, scale);
+        else                      d2 = 0.5 * (qat(ne, vi + 1, scale) - qat(ne, vi - 1, scale));
+        if (F64OUT) {
+            double2* o = reinterpret_cast<double2*>(out) + 2 * vi;
+            o[0] = make_double2(q, d0);
+            o[1] = make_double2(d1, d2);
+        } else {
+            reinterpret_cast<float4*>(out)[vi] = make_float4((float)q, (float)d0, (float)d1, (float)d2);
+        }
+    }
+}
+
+template <class P>
+__global__ void __launch_bounds__(256) sample_kernel(const void* __restrict__ grid, GridGeo g,
+                                                     double o0, double o1, double o2,
+                                                     double ih0, double ih1, double ih2,
+                                                     const double* __restrict__ pts, long long n,
+                                                     typename P::R* __restrict__ out) {
+    using R = typename P::R;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const R px = (R)((pts[i] - o0) * ih0);
+        const R py = (R)((pts[n + i] - o1) * ih1);
+        const R pz = (R)((pts[2 * n + i] - o2) * ih2);
+        typename P::V v;
+        sample<P>(grid, g, px, py, pz, v);
+        out[i] = v.x;
+        out[n + i] = v.y;
+        out[2 * n + i] = v.z;
+        out[3 * n + i] = v.w;
+    }
+}
+
+static int grid_blocks(long long work, int per_sm) {
+    int sms = 148;
+    if (device_sm_count(&sms) != SLOTH_OK) sms = 148;
+    long long b = (work + 255) / 256;
+    long long cap = (long long)sms * per_sm;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+template <bool F64OUT>
+static int pack_impl(const SlothGridDesc* g, const void* ne, int ne_is_f64, double ne_scale,
+                     void* grid_out, void* stream) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (!ne || !grid_out) return SLOTH_ERR_NULL_POINTER;
+    if (!(ne_scale > 0.0) || !std::isfinite(ne_scale)) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (((uintptr_t)grid_out & 15u) != 0) return SLOTH_ERR_MISALIGNED;
+    if (((uintptr_t)ne & (ne_is_f64 ? 7u : 3u)) != 0) return SLOTH_ERR_MISALIGNED;
+    const GridGeo geo = make_geo(g);
+    const long long total = (long long)g->n[0] * g->n[1] * g->n[2];
+    cudaStream_t s = (cudaStream_t)stream;
+    const int blocks = grid_blocks(total, 16);
+    if (ne_is_f64)
+        pack_kernel<double, F64OUT><<<blocks, 256, 0, s>>>((const double*)ne, grid_out, geo, ne_scale, total);
+    else
+        pack_kernel<float, F64OUT><<<blocks, 256, 0, s>>>((const float*)ne, grid_out, geo, ne_scale, total);
+    note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+template <class P>
+static int sample_impl(const SlothGridDesc* g, const void* grid, const double* points, int64_t n,
+                       typename P::R* out, void* stream) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (n < 0) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (n == 0) return SLOTH_OK;
+    if (!grid || !points || !out) return SLOTH_ERR_NULL_POINTER;
+    if (((uintptr_t)grid & 15u) != 0) return SLOTH_ERR_MISALIGNED;
+    const GridGeo geo = make_geo(g);
+    cudaStream_t s = (cudaStream_t)stream;
+    sample_kernel<P><<<grid_blocks(n, 8), 256, 0, s>>>(
+        grid, geo, g->origin[0], g->origin[1], g->origin[2], 1.0 / g->spacing[0], 1.0 / g->spacing[1],
+        1.0 / g->spacing[2], points, (long long)n, out);
+    note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+}  // namespace sloth
+
+extern "C" {
+
+size_t sloth_grid_bytes(const SlothGridDesc* g, int real_bytes) {
+    if (sloth::check_grid(g) != SLOTH_OK) return 0;
+    if (real_bytes != 4 && real_bytes != 8) return 0;
+    return (size_t)g->n[0] * (size_t)g->n[1] * (size_t)g->n[2] * 4u * (size_t)real_bytes;
+}
+
+int sloth_grid_pack_f32(const SlothGridDesc* g, const void* ne, int ne_is_f64, double ne_scale,
+                        void* grid_out, void* stream) {
+    return sloth::pack_impl<false>(g, ne, ne_is_f64, ne_scale, grid_out, stream);
+}
+
+int sloth_grid_pack_f64(const SlothGridDesc* g, const void* ne, int ne_is_f64, double ne_scale,
+                        void* grid_out, void* stream) {
+    return sloth::pack_impl<true>(g, ne, ne_is_f64, ne_scale, grid_out, stream);
+}
+
+int sloth_sample_f32(const SlothGridDesc* g, const void* grid, const double* points, int64_t n,
+                     float* out, void* stream) {
+    return sloth::sample_impl<sloth::PolF32>(g, grid, points, n, out, stream);
+}
+
+int sloth_sample_f64(const SlothGridDesc* g, const void* grid, const double* points, int64_t n,
+                     double* out, void* stream) {
+    return sloth::sample_impl<sloth::PolF64>(g, grid, points, n, out, stream);
+}
+
+}  // extern "C"

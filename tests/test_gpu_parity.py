@@ -1,0 +1,169 @@
+"""Parity of the CUDA kernels (through the C ABI) with the oracle on seeded inputs.
+
+Tolerances (stated for every output):
+* FP64 kernel vs FP64 oracle: positions 1e-10 of the box length, directions
+  1e-10 (|d(v/c)|), phase 1e-10 relative, amplitude 1e-12 absolute.
+* FP32 split kernel vs FP64 oracle: positions 1e-6 of the box length,
+  directions 1e-6, phase 1e-6 relative (of max |phase|), amplitude 1e-6 absolute.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+from helpers import C, case, direction_error, position_error, run_kernel, run_oracle
+from oracle import ref_restated as rr
+from sloth_b200 import _capi, runtime
+
+pytestmark = pytest.mark.gpu
+
+L = 5e-3
+
+
+@pytest.mark.parametrize("ne_dtype", [np.float32, np.float64])
+def test_pack_matches_oracle_bitwise(ne_dtype):
+    rng = np.random.RandomState(5)
+    ne = rng.uniform(1e24, 3e25, size=(9, 10, 11)).astype(ne_dtype)
+    omega = 2 * np.pi * C / 532e-9
+    scale = 1.0 / rr.critical_density(omega)
+    ref = rr.pack_grid(ne.astype(np.float64), scale)
+    g64 = runtime.pack_grid(torch.from_numpy(ne), (0, 0, 0), (1e-5,) * 3, omega, precision="f64")
+    np.testing.assert_array_equal(g64.data.view(9, 10, 11, 4).cpu().numpy(), ref)
+    g32 = runtime.pack_grid(torch.from_numpy(ne), (0, 0, 0), (1e-5,) * 3, omega, precision="f32")
+    np.testing.assert_array_equal(g32.data.view(9, 10, 11, 4).cpu().numpy(), ref.astype(np.float32))
+
+
+@pytest.mark.parametrize("precision,rtol", [("f64", 1e-13), ("f32", 2e-6)])
+def test_sample_matches_reference_interpolator(precision, rtol):
+    g = golden("interpolator")
+    x, y, z = g["x"], g["y"], g["z"]
+    origin = (x[0], y[0], z[0])
+    spacing = tuple((a[-1] - a[0]) / (a.size - 1) for a in (x, y, z))
+    grid = runtime.pack_grid(torch.from_numpy(g["values"]), origin, spacing, 1.0, precision=precision, ne_scale=1.0)
+    got = runtime.sample(grid, g["points"].T)[0].cpu().numpy().astype(np.float64)
+    scale = np.abs(g["values"]).max()
+    np.testing.assert_allclose(got, g["result"], rtol=0, atol=rtol * scale)
+    out = (g["points"][:, 0] < x[0]) | (g["points"][:, 0] > x[-1])
+    assert (got[out] == 0).all()
+
+
+CASES = [
+    # kind, n, nrays, axis, inv_brems, project, n_saves, jitter
+    ("sinusoid", 64, 3000, 2, False, False, 1, 0.0),
+    ("trough", 48, 2000, 2, True, True, 1, 1e-3),
+    ("kolmogorov", 40, 2000, 2, True, False, 4, 0.0),
+    ("kolmogorov", 32, 1500, 0, False, True, 1, 2e-3),
+    ("sinusoid", 32, 1500, 1, True, False, 3, 5e-3),
+]
+
+
+def _sched(n, n_saves, solve_like):
+    h = L / (n - 1)
+    if solve_like:
+        taus = np.array([np.sqrt(8.0) * L])
+    else:
+        taus = np.linspace(0.0, L, n_saves)
+    return runtime.schedule_times(taus, (h, h, h))
+
+
+def _run_pair(kind, n, nrays, axis, ib, project, n_saves, jitter, precision):
+    ne, rays, origin, spacing, omega = case(kind, n, nrays, axis=axis, jitter=jitter, seed=n + axis)
+    sched = _sched(n, n_saves, n_saves == 1)
+    Te, Z = (20.0, 1.0) if ib else (None, None)
+    kw = dict(axis=axis, project=project, plane=L / 2, inv_brems=ib, Te=Te, Z=Z)
+    k = run_kernel(ne, rays, origin, spacing, omega, sched, precision=precision, **kw)
+    o = run_oracle(ne, rays, origin, spacing, omega, sched, **kw)
+    return k, o
+
+
+@pytest.mark.parametrize("kind,n,nrays,axis,ib,project,n_saves,jitter", CASES)
+def test_trace_f64_matches_oracle(kind, n, nrays, axis, ib, project, n_saves, jitter):
+    k, o = _run_pair(kind, n, nrays, axis, ib, project, n_saves, jitter, "f64")
+    assert position_error(k["state"], o["state"], L) < 1e-10
+    assert direction_error(k["state"], o["state"]) < 1e-10
+    np.testing.assert_allclose(k["jones"][:, [0, 2]], o["jones"][:, [0, 2]], rtol=0, atol=1e-10 * L)
+    np.testing.assert_allclose(k["jones"][:, [1, 3]], o["jones"][:, [1, 3]], rtol=0, atol=1e-10)
+    ph = np.abs(o["phase"]).max()
+    np.testing.assert_allclose(k["phase"], o["phase"], rtol=0, atol=1e-10 * max(ph, 1e-30))
+    if ib:
+        np.testing.assert_allclose(k["amp"], o["amp"], rtol=0, atol=1e-12)
+    assert (k["steps"] != o["steps"]).mean() < 1e-3
+    assert (k["status"] != o["status"]).mean() < 1e-3
+    assert k["total_steps"] == int(k["steps"].astype(np.int64).sum())
+
+
+@pytest.mark.parametrize("kind,n,nrays,axis,ib,project,n_saves,jitter", CASES)
+def test_trace_f32_within_tolerance(kind, n, nrays, axis, ib, project, n_saves, jitter):
+    k, o = _run_pair(kind, n, nrays, axis, ib, project, n_saves, jitter, "f32")
+    pe = position_error(k["state"], o["state"], L)
+    de = direction_error(k["state"], o["state"])
+    assert pe < 1e-6, pe
+    assert de < 1e-6, de
+    ph = np.abs(o["phase"]).max()
+    assert np.abs(k["phase"] - o["phase"]).max() <= 1e-6 * max(ph, 1e-30)
+    if ib:
+        assert np.abs(k["amp"].astype(np.float64) - o["amp"]).max() < 1e-6
+    assert (k["steps"] != o["steps"]).mean() < 5e-3
+
+
+def test_order_invariance_bitwise():
+    """Each ray's result is independent of the order and company it is traced in."""
+    ne, rays, origin, spacing, omega = case("kolmogorov", 40, 4000, seed=11)
+    sched = _sched(40, 3, False)
+    a = run_kernel(ne, rays, origin, spacing, omega, sched, precision="f32", inv_brems=True, Te=20.0, Z=1.0)
+    perm = np.random.RandomState(0).permutation(rays.shape[1])
+    sub = perm[:1234]
+    b = run_kernel(ne, np.ascontiguousarray(rays[:, sub]), origin, spacing, omega, sched, precision="f32",
+                   inv_brems=True, Te=20.0, Z=1.0)
+    for key in ("jones", "state", "phase", "amp"):
+        np.testing.assert_array_equal(b[key][..., :], a[key][..., sub])
+    np.testing.assert_array_equal(b["steps"], a["steps"][sub])
+
+
+def test_rays_starting_outside():
+    """Rays outside the grid: receding ones leave at once, approaching ones drift in."""
+    ne, rays, origin, spacing, omega = case("sinusoid", 32, 8)
+    rays = rays.astype(np.float64)
+    rays[0, 0] = 3e-3          # outside in x, moving along z only -> never enters
+    rays[2, 1] = -4e-3         # 1.5 mm before the entry face -> drifts in
+    rays[5, 2] = -C            # on the entry face moving backwards -> leaves at once
+    rays[0, 3], rays[3, 3] = -2.6e-3, 0.01 * C   # outside in x, moving towards the grid
+    rays[5, 3] = C * np.sqrt(1 - 0.01 ** 2)
+    rays = rays.astype(np.float32)
+    sched = _sched(32, 3, False)
+    for precision in ("f64", "f32"):
+        k = run_kernel(ne, rays, origin, spacing, omega, sched, precision=precision)
+        o = run_oracle(ne, rays, origin, spacing, omega, sched)
+        assert position_error(k["state"], o["state"], L) < (1e-10 if precision == "f64" else 1e-6)
+        np.testing.assert_array_equal(k["steps"], o["steps"])
+        assert k["steps"][0] == 0 and k["steps"][2] <= 1   # ray 2 leaves through a zero-length clipped step
+        assert k["steps"][1] > 0
+
+
+def test_empty_single_and_vacuum():
+    ne, rays, origin, spacing, omega = case("vacuum", 16, 5)
+    sched = _sched(16, 2, False)
+    k = run_kernel(ne, rays, origin, spacing, omega, sched, precision="f32")
+    np.testing.assert_allclose(k["state"][-1, :2], rays[:2], rtol=0, atol=1e-9)
+    assert (k["phase"] == 0).all()
+    one = run_kernel(ne, np.ascontiguousarray(rays[:, :1]), origin, spacing, omega, sched, precision="f64")
+    assert one["jones"].shape == (2, 4, 1)
+    g = runtime.pack_grid(torch.from_numpy(ne), origin, spacing, omega)
+    out = runtime.trace(g, torch.zeros((6, 0), device="cuda"), sched)
+    torch.cuda.synchronize()
+    assert out["jones"].shape == (2, 4, 0) and int(out["total_steps"][0]) == 0
+
+
+def test_error_codes_from_device_entry_points():
+    ne, rays, origin, spacing, omega = case("sinusoid", 16, 64)
+    g = runtime.pack_grid(torch.from_numpy(ne), origin, spacing, omega)
+    r = torch.from_numpy(rays).cuda()
+    sched = _sched(16, 1, True)
+    small = torch.empty(1024, dtype=torch.uint8, device="cuda")
+    with pytest.raises(_capi.SlothError) as e:
+        runtime.trace(g, r, sched, workspace=small)
+    assert e.value.code == _capi.SLOTH_ERR_WORKSPACE_TOO_SMALL
+    bad = torch.empty(g.data.numel() + 4, dtype=torch.float32, device="cuda")[1:]
+    with pytest.raises(_capi.SlothError) as e:
+        runtime.pack_grid(torch.from_numpy(ne), origin, spacing, omega, out=bad)
+    assert e.value.code == _capi.SLOTH_ERR_MISALIGNED
