@@ -311,6 +311,9 @@ def run_sloth(args):
         # accuracy of the FP32 split kernel against the FP64 port (all rays)
         j32, j64 = f32_out["jones"][-1].double(), o64["jones"][-1]
         ok = (f32_out["status"] != 2) & (o64["status"] != 2)
+        # rays that crossed the far face inside the box's transverse extent;
+        # the others left (or never entered) through a side face at grazing incidence
+        far = ok & (j64[0].abs() <= L / 2) & (j64[2].abs() <= L / 2)
         dpos = torch.maximum((j32[0] - j64[0]).abs(), (j32[2] - j64[2]).abs())[ok] / L
         dang = torch.maximum((j32[1] - j64[1]).abs(), (j32[3] - j64[3]).abs())[ok]
         ph64 = o64["phase"][-1][ok]
@@ -320,11 +323,16 @@ def run_sloth(args):
         def q(t, p):
             t = t.float() if t.numel() < 2 ** 24 else t[:: max(1, t.numel() // 2 ** 23)].float()
             return float(torch.quantile(t, p))
+        farm = far[ok]
         acc = {"position_rel_L_max": float(dpos.max()), "position_rel_L_p99": q(dpos, 0.99),
                "angle_abs_max_rad": float(dang.max()), "angle_abs_p99_rad": q(dang, 0.99),
                "phase_abs_max_rad": float(dph.max()), "phase_max_abs_rad": float(ph64.abs().max()),
                "phase_rel_max": float(dph.max() / ph64.abs().max()),
-               "amp_abs_max": float(damp.max()), "rays_compared": int(ok.sum()),
+               "phase_rel_max_far_face": float(dph[farm].max() / ph64.abs().max()),
+               "phase_rel_p99": q(dph / ph64.abs().max(), 0.99),
+               "amp_abs_max": float(damp.max()), "amp_abs_max_far_face": float(damp[farm].max()),
+               "amp_abs_p99": q(damp, 0.99),
+               "rays_compared": int(ok.sum()), "rays_far_face": int(farm.sum()),
                "status_mismatch": int((f32_out["status"] != o64["status"]).sum())}
         del g64, r64, o64
 

@@ -79,6 +79,9 @@ typedef struct SlothTraceParams {
                                  out (1/m): 3.1e-5*Z*(nc_cc/omega)^2*Te^-1.5        */
     double  coulomb_log_w;    /* ln(v_the/(omega*b_min)): Coulomb log for ne < nc   */
     double  ope_ratio2;       /* (omega_pe/omega)^2 per unit ne/nc (NRL constants)  */
+    double  q_max;            /* upper bound of ne/nc over the grid, or 0 if unknown;
+                                 a bound selects faster exact paths (sub-critical
+                                 kappa; series n - 1 when (omega_pe/omega)^2 <= 0.05) */
 } SlothTraceParams;
 
 #define SLOTH_MAX_SAVES 4096

@@ -24,6 +24,7 @@
 #include <unistd.h>
 
 #define ORACLE_C 299792458.0
+#define FACE_MARGIN 0.02   /* cells: steps ending this close to a face sample the inside limit */
 
 typedef struct {
     int32_t n[3];
@@ -87,8 +88,14 @@ static double phase_rate(double ne, double omega) {
     return -omega * x / (1.0 + sqrt(om));
 }
 
-static void rhs(const OracleParams* p, const double r[3], double a[3], double* g, double* k) {
+static void rhs(const OracleParams* p, const double r_in[3], int clip, double a[3], double* g, double* k) {
     Samp s;
+    double r[3] = {r_in[0], r_in[1], r_in[2]};
+    if (clip)   /* a step cut at a face samples the field's limit from inside */
+        for (int d = 0; d < 3; ++d) {
+            const double lo = p->origin[d], hi = p->origin[d] + p->spacing[d] * (double)(p->n[d] - 1);
+            r[d] = r[d] < lo ? lo : (r[d] > hi ? hi : r[d]);
+        }
     sample(p, r, &s);
     a[0] = s.f[1];
     a[1] = s.f[2];
@@ -141,25 +148,25 @@ static int inside(const OracleParams* p, const double r[3]) {
 }
 
 /* One RK4 step of length h (seconds) of r' = v, v' = grad G, phase, tau. */
-static void rk4(const OracleParams* p, double h, double r[3], double v[3], double* ph, double* ta) {
+static void rk4(const OracleParams* p, double h, int clip, double r[3], double v[3], double* ph, double* ta) {
     double a1[3], a2[3], a3[3], a4[3], r2[3], v2[3], r3[3], v3[3], r4[3], v4[3];
     double g1, g2, g3, g4, k1, k2, k3, k4;
-    rhs(p, r, a1, &g1, &k1);
+    rhs(p, r, clip, a1, &g1, &k1);
     for (int a = 0; a < 3; ++a) {
         r2[a] = r[a] + 0.5 * h * v[a];
         v2[a] = v[a] + 0.5 * h * a1[a];
     }
-    rhs(p, r2, a2, &g2, &k2);
+    rhs(p, r2, clip, a2, &g2, &k2);
     for (int a = 0; a < 3; ++a) {
         r3[a] = r[a] + 0.5 * h * v2[a];
         v3[a] = v[a] + 0.5 * h * a2[a];
     }
-    rhs(p, r3, a3, &g3, &k3);
+    rhs(p, r3, clip, a3, &g3, &k3);
     for (int a = 0; a < 3; ++a) {
         r4[a] = r[a] + h * v3[a];
         v4[a] = v[a] + h * a3[a];
     }
-    rhs(p, r4, a4, &g4, &k4);
+    rhs(p, r4, clip, a4, &g4, &k4);
     for (int a = 0; a < 3; ++a) {
         r[a] += h / 6.0 * (v[a] + 2.0 * v2[a] + 2.0 * v3[a] + v4[a]);
         v[a] += h / 6.0 * (a1[a] + 2.0 * a2[a] + 2.0 * a3[a] + a4[a]);
@@ -210,10 +217,13 @@ static long long trace_one(const OracleParams* p, const double* rays, int64_t n,
         if (frozen_t < 0.0 && p->early_exit && gone(p, r, v)) frozen_t = (double)step;
         if (frozen_t < 0.0) {
             double phi = 1.0;
+            int near = 0;
             if (inside(p, r)) {
                 for (int a = 0; a < 3; ++a) {
                     const double lo = p->origin[a], hi = p->origin[a] + p->spacing[a] * (double)(p->n[a] - 1);
                     const double pn = r[a] + v[a] * dt;
+                    const double marg = FACE_MARGIN * p->spacing[a];
+                    if (pn > hi - marg || pn < lo + marg) near = 1;
                     if (pn > hi) {
                         const double t = (hi - r[a]) / (v[a] * dt);
                         if (t < phi) phi = t;
@@ -226,7 +236,7 @@ static long long trace_one(const OracleParams* p, const double* rays, int64_t n,
             }
             const int split = phi < 1.0;
             if (phi < 0.0) phi = 0.0;
-            rk4(p, dt * phi, r, v, &ph, &ta);
+            rk4(p, dt * phi, split || near, r, v, &ph, &ta);
             ++nst;
             if (split) frozen_t = (double)step + phi;
         }

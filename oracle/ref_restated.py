@@ -34,6 +34,7 @@ from scipy.constants import e as E_CHARGE
 from scipy.constants import epsilon_0 as EPS0
 
 ALPHA = 3.14207787e-4   # m_e * eps0 / e^2, the reference's constant (propagator.py:73, :88)
+FACE_MARGIN = 0.02      # cells: steps ending this close to a face sample the inside limit
 
 
 # ---------------------------------------------------------------------------
@@ -278,8 +279,11 @@ def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=
     phi = the smallest positive (face - r)/(v*dt)); the ray is then frozen and
     advanced to later saves by straight-line drift from its exit time. A ray
     outside the grid on an axis and moving away on it is frozen likewise.
-    With early_exit=False frozen rays are instead stepped with the zero RHS
-    (which is the same drift). kappa is the reference's interpolated kappa
+    The last stage point of such a clipped step lies on the face up to
+    O(h^2 * acceleration), where the RHS jumps, so the clipped step, and any
+    step whose prediction ends within FACE_MARGIN cells of a face, samples its
+    stage points clamped into the grid box: it integrates the field's limit
+    from inside, as an event-locating adaptive solver does. kappa is the reference's interpolated kappa
     grid; phase_mode 'kernel' takes n from the interpolated density,
     'reference' interpolates the (n - 1) grid (full_solver.py:289).
     Returns a dict of arrays.
@@ -302,7 +306,11 @@ def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=
     lo = grid.origin
     hi = grid.origin + grid.spacing * (np.asarray(grid.n) - 1)
 
-    def rhs(rr):
+    def rhs(rr, clip=None):
+        if clip is not None and clip.any():
+            rr = rr.copy()
+            for a in range(3):
+                rr[a] = np.where(clip, np.clip(rr[a], lo[a], hi[a]), rr[a])
         f, k, m = grid.sample(rr, with_kappa=inv_brems, with_nm1=(phase_mode == "reference"))
         a = f[:, 1:].T
         if phase_mode == "reference":
@@ -352,24 +360,28 @@ def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=
             rr, vv = r[:, idx], v[:, idx]
             # shorten the step of rays that would leave the grid within it
             phi = np.ones(idx.size)
+            near = np.zeros(idx.size, dtype=bool)
             ins = inside(rr)
             for a in range(3):
                 pn = rr[a] + vv[a] * dt
+                marg = FACE_MARGIN * grid.spacing[a]
+                near |= ins & ((pn > hi[a] - marg) | (pn < lo[a] + marg))
                 with np.errstate(divide="ignore", invalid="ignore"):
                     up = ins & (pn > hi[a])
                     phi = np.where(up, np.minimum(phi, (hi[a] - rr[a]) / (vv[a] * dt)), phi)
                     dn = ins & (pn < lo[a])
                     phi = np.where(dn, np.minimum(phi, (lo[a] - rr[a]) / (vv[a] * dt)), phi)
             split = phi < 1.0
+            clamp = split | near
             phi = np.maximum(phi, 0.0)
             h = dt * phi
-            a1, g1, k1 = rhs(rr)
+            a1, g1, k1 = rhs(rr, clamp)
             r2, v2 = rr + 0.5 * h * vv, vv + 0.5 * h * a1
-            a2, g2, k2 = rhs(r2)
+            a2, g2, k2 = rhs(r2, clamp)
             r3, v3 = rr + 0.5 * h * v2, vv + 0.5 * h * a2
-            a3, g3, k3 = rhs(r3)
+            a3, g3, k3 = rhs(r3, clamp)
             r4, v4 = rr + h * v3, vv + h * a3
-            a4, g4, k4 = rhs(r4)
+            a4, g4, k4 = rhs(r4, clamp)
             r[:, idx] = rr + h / 6.0 * (vv + 2 * v2 + 2 * v3 + v4)
             v[:, idx] = vv + h / 6.0 * (a1 + 2 * a2 + 2 * a3 + a4)
             phase[idx] += h / 6.0 * (g1 + 2 * g2 + 2 * g3 + g4)
@@ -379,8 +391,6 @@ def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=
                 sidx = idx[split]
                 frozen_t[sidx] = step + phi[split]
                 alive[sidx] = False
-        if not early_exit:
-            pass  # frozen rays drift exactly; stepping them with a zero RHS changes nothing
         step += 1
         if step > last:
             break

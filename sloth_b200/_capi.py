@@ -14,7 +14,8 @@ from ctypes import (POINTER, Structure, c_char_p, c_double, c_int, c_int32, c_in
                     c_size_t, c_uint8, c_ulonglong, c_void_p)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libsloth_b200.so")
+# SLOTH_B200_LIB selects another build of the same library (e.g. a tuning variant).
+LIB_PATH = os.environ.get("SLOTH_B200_LIB") or os.path.join(_HERE, "_lib", "libsloth_b200.so")
 
 SLOTH_OK = 0
 SLOTH_ERR_INVALID_ARGUMENT = -1
@@ -59,7 +60,7 @@ class SlothTraceParams(Structure):
                 ("first_save", c_int32), ("save_every", c_int32), ("n_saves", c_int32),
                 ("probing_axis", c_int32), ("project_to_plane", c_int32), ("inv_brems", c_int32),
                 ("plane", c_double), ("kappa_q2", c_double), ("coulomb_log_w", c_double),
-                ("ope_ratio2", c_double)]
+                ("ope_ratio2", c_double), ("q_max", c_double)]
 
 
 class SlothTraceOutputs(Structure):

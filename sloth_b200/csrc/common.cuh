@@ -18,7 +18,6 @@
 namespace sloth {
 
 constexpr double kC = 299792458.0;          // speed of light (scipy.constants.c)
-constexpr int kTraceThreads = 256;          // threads per tracer CTA
 constexpr int kTile = 1024;                 // rays per shared-memory sorted tile
 constexpr int kMaxBucketBits = 18;          // at most 2^18 Morton buckets
 
@@ -80,10 +79,19 @@ struct AccD {
 struct Vox4F { float x, y, z, w; };
 struct Vox4D { double x, y, z, w; };
 
+#ifndef SLOTH_CELL_CACHE_F32
+#define SLOTH_CELL_CACHE_F32 1
+#endif
+#ifndef SLOTH_CELL_CACHE_F64
+#define SLOTH_CELL_CACHE_F64 1
+#endif
+
 struct PolF32 {
     using R = float;
     using V = Vox4F;
     using Acc = AccF;
+    // keep the last cell's 8 corners in registers across stages and steps
+    static constexpr bool cell_cache = SLOTH_CELL_CACHE_F32 != 0;
     __device__ __forceinline__ static V load(const void* g, unsigned i) {
         const float4 v = __ldg(reinterpret_cast<const float4*>(g) + i);
         return V{v.x, v.y, v.z, v.w};
@@ -102,6 +110,7 @@ struct PolF64 {
     using R = double;
     using V = Vox4D;
     using Acc = AccD;
+    static constexpr bool cell_cache = SLOTH_CELL_CACHE_F64 != 0;
     __device__ __forceinline__ static V load(const void* g, unsigned i) {
         const double2* p = reinterpret_cast<const double2*>(g) + 2u * (size_t)i;
         const double2 a = __ldg(p), b = __ldg(p + 1);

@@ -11,9 +11,12 @@
 
 namespace sloth {
 
+// q = ne * scale, rounded on its own (__dmul_rn keeps the compiler from
+// fusing it into the differences below, so the result is bit-identical to a
+// plain IEEE evaluation of the same formula).
 template <class In>
 __device__ __forceinline__ double qat(const In* __restrict__ ne, size_t i, double scale) {
-    return (double)__ldg(ne + i) * scale;
+    return __dmul_rn((double)__ldg(ne + i), scale);
 }
 
 template <class In, bool F64OUT>

@@ -13,6 +13,13 @@
 // and the inverse-bremsstrahlung optical depth, both as RK4 quadratures of
 // the stage values, and the Jones-vector projection at each save.
 //
+// Grid faces: the RHS jumps to the outside fill there. A step whose
+// straight-line prediction p + w crosses a face is cut to end on it (RK4 with
+// a fraction phi of the step) and the ray then leaves on a straight line; a
+// step whose prediction ends within kFaceMargin cells of a face, or is cut,
+// samples its stage points clamped into the grid, i.e. it integrates the
+// field's limit from inside, so that no stage sits on the discontinuity.
+//
 // Launch structure (all on the caller's stream):
 //   1. keys_kernel   : Morton key of each ray's entry cell + bucket histogram
 //   2. scan_kernel   : exclusive scan of the bucket counts (one CTA)
@@ -26,7 +33,21 @@
 
 #include "common.cuh"
 
+#ifndef SLOTH_TRACE_THREADS
+#define SLOTH_TRACE_THREADS 256
+#endif
+#ifndef SLOTH_TRACE_MIN_BLOCKS
+#define SLOTH_TRACE_MIN_BLOCKS 2
+#endif
+
 namespace sloth {
+
+constexpr int kThreads = SLOTH_TRACE_THREADS;
+constexpr double kFaceMargin = 0.02;     // cells
+constexpr double kSmallX = 0.05;         // bound on (omega_pe/omega)^2 for the series form of n - 1
+
+// Inverse-bremsstrahlung modes of the tracer.
+enum { IB_OFF = 0, IB_SUBCRITICAL = 1, IB_GENERAL = 2 };
 
 // ---------------------------------------------------------------------------
 // Kernel arguments.
@@ -51,7 +72,7 @@ struct TraceArgs {
     double plane;
     int first_save, save_every, n_saves;
     int axis, t1, t2;
-    int project, inv_brems;
+    int project;
     void* jones;
     void* state;
     double* phase;
@@ -83,44 +104,83 @@ struct CellCache {
     typename P::V c[8];
 };
 
-// Trilinear sample of the packed grid (same rules as sample() in
-// common.cuh, after src/core/interpolator.py:79-104) returning q, the three
-// gradient channels and, when IB, the interpolated inverse-bremsstrahlung
-// rate per kappa_q2. The reference interpolates a kappa grid computed at the
-// grid points (src/core/propagator.py:239, :623-631); with uniform Te and Z
-// that grid is q^2 * CL(q) per point, so its interpolant is the weighted sum
-// of the corner values, formed here from the corners already loaded.
-// CL(q) = max(2, cl_w - ln(max(omega_pe/omega, 1))) is constant below the
-// critical density; corners above it take the logarithm.
-// With CACHE the 8 corners of the last cell stay in registers and are
-// reloaded only when the cell changes.
 template <class P>
 struct Sample {
     typename P::R q, g0, g1, g2, k;
 };
 
-template <class P, bool IB>
-__device__ __forceinline__ typename P::R corner_kappa(const TraceArgs& a, typename P::R q);
+// n - 1 for n = sqrt(1 - x), x = (omega_pe/omega)^2. SMALLX (FP32 only, used
+// when x <= kSmallX over the whole grid) takes the binomial series
+// -(x/2 + x^2/8 + x^3/16 + 5x^4/128 + 7x^5/256), whose first omitted term is
+// below 2e-8 of x/2 there, instead of a square root and a division.
+template <class P, bool SMALLX>
+__device__ __forceinline__ typename P::R nm1(typename P::R x) {
+    using R = typename P::R;
+    if constexpr (SMALLX && sizeof(R) == 4) {
+        return -x * (R(0.5) + x * (R(0.125) + x * (R(0.0625) + x * (R(0.0390625) + x * R(0.02734375)))));
+    } else {
+        return P::n_minus_1(x);
+    }
+}
 
-template <class P, bool CACHE, bool IB>
-__device__ __forceinline__ void sample_c(const TraceArgs& a, typename P::R px, typename P::R py,
-                                         typename P::R pz, Sample<P>& out, CellCache<P>& cc) {
+// Inverse-bremsstrahlung rate of one grid point per kappa_q2: q^2 * CL(q),
+// CL = max(2, cl_w - ln(max(omega_pe/omega, 1))) (src/core/propagator.py:155-162).
+template <class P>
+__device__ __forceinline__ typename P::R corner_kappa(const TraceArgs& a, typename P::R q) {
+    using R = typename P::R;
+    const R x = q * (R)a.ope2;
+    const R cl = (x > R(1)) ? fmax(R(2), (R)a.cl_w - R(0.5) * P::log_(x)) : (R)a.cl_lo;
+    return q * q * cl;
+}
+
+// Trilinear sample of the packed grid (rules of src/core/interpolator.py:79-104:
+// cell i = floor(p) clamped to [0, n-2], product weights, fill 0 outside)
+// returning q, the three gradient channels and, when IB, the interpolated
+// inverse-bremsstrahlung rate per kappa_q2. The reference interpolates a
+// kappa grid computed at the grid points (src/core/propagator.py:239,
+// :623-631); with uniform Te and Z that grid is q^2 * CL(q) per point, so its
+// interpolant is the weighted sum of the corner values, formed here from the
+// corners already loaded (CL is constant below the critical density).
+//
+// The point is hi + lo: hi is the ray's running position (large) and lo its
+// compensation plus the stage offset (small). The cell index comes from the
+// rounded sum; the weights from (hi - i) + lo, which resolves the position
+// inside the cell to FP32 relative precision rather than FP32 precision of
+// the absolute position. CLAMP moves the point into the grid first.
+template <class P, int IB, bool CLAMP>
+__device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R (&hi)[3],
+                                         const typename P::R (&lo)[3], Sample<P>& out, CellCache<P>& cc) {
     using R = typename P::R;
     using V = typename P::V;
     const GridGeo& g = a.geo;
-    const bool in = (px >= R(0)) & (px <= lim_of<R>(g, 0)) & (py >= R(0)) &
-                    (py <= lim_of<R>(g, 1)) & (pz >= R(0)) & (pz <= lim_of<R>(g, 2));
+    R h[3], l[3], p[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        h[x] = hi[x];
+        l[x] = lo[x];
+        p[x] = h[x] + l[x];
+        if constexpr (CLAMP) {
+            const R pc = fmin(fmax(p[x], R(0)), lim_of<R>(g, x));
+            if (pc != p[x]) {
+                h[x] = pc;
+                l[x] = R(0);
+                p[x] = pc;
+            }
+        }
+    }
+    const bool in = (p[0] >= R(0)) & (p[0] <= lim_of<R>(g, 0)) & (p[1] >= R(0)) &
+                    (p[1] <= lim_of<R>(g, 1)) & (p[2] >= R(0)) & (p[2] <= lim_of<R>(g, 2));
     if (!in) {
         out.q = out.g0 = out.g1 = out.g2 = out.k = R(0);
         return;
     }
-    const int ix = min((int)px, g.n[0] - 2);
-    const int iy = min((int)py, g.n[1] - 2);
-    const int iz = min((int)pz, g.n[2] - 2);
-    const R fx = px - (R)ix, fy = py - (R)iy, fz = pz - (R)iz;
+    const int ix = min((int)p[0], g.n[0] - 2);
+    const int iy = min((int)p[1], g.n[1] - 2);
+    const int iz = min((int)p[2], g.n[2] - 2);
+    const R fx = (h[0] - (R)ix) + l[0], fy = (h[1] - (R)iy) + l[1], fz = (h[2] - (R)iz) + l[2];
     const unsigned b = (unsigned)ix * g.sx + (unsigned)iy * g.sy + (unsigned)iz;
     V c[8];
-    if constexpr (CACHE) {
+    if constexpr (P::cell_cache) {
         if (b != cc.base) {
             cc.base = b;
             cc.c[0] = P::load(a.grid, b);
@@ -159,66 +219,58 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, typename P::R px, t
     out.g0 = g0;
     out.g1 = g1;
     out.g2 = g2;
-    if constexpr (IB) {
-        R qmax = c[0].x, k = R(0);
+    if constexpr (IB == IB_SUBCRITICAL) {
+        R k = R(0);
 #pragma unroll
-        for (int i = 1; i < 8; ++i) qmax = fmax(qmax, c[i].x);
-        if (qmax * (R)a.ope2 > R(1)) {
+        for (int i = 0; i < 8; ++i) k += w[i] * (c[i].x * c[i].x);
+        out.k = k * (R)a.cl_lo;
+    } else if constexpr (IB == IB_GENERAL) {
+        R k = R(0);
 #pragma unroll
-            for (int i = 0; i < 8; ++i) k += w[i] * corner_kappa<P, IB>(a, c[i].x);
-        } else {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) k += w[i] * (c[i].x * c[i].x);
-            k *= (R)a.cl_lo;
-        }
+        for (int i = 0; i < 8; ++i) k += w[i] * corner_kappa<P>(a, c[i].x);
         out.k = k;
     } else {
         out.k = R(0);
     }
 }
 
-template <class P, bool IB>
-__device__ __forceinline__ typename P::R corner_kappa(const TraceArgs& a, typename P::R q) {
-    using R = typename P::R;
-    const R x = q * (R)a.ope2;
-    const R cl = (x > R(1)) ? fmax(R(2), (R)a.cl_w - R(0.5) * P::log_(x)) : (R)a.cl_lo;
-    return q * q * cl;
-}
-
-// One RK4 step of length phi (in steps; phi = 1 except for a step clipped
-// at a grid face) in scaled units; see the file header. Stage sums are
+// One RK4 step of length phi (in steps; phi = 1 except for a step cut at a
+// grid face) in scaled units; see the file header. Stage sums are
 // accumulated as the stages are produced to keep few values live:
 //   p' = p + phi*w + phi^2 (A1 + A2 + A3)/6,  w' = w + phi (A1 + 2A2 + 2A3 + A4)/6,
 //   stage points p, p + phi*w/2, p + phi*w2/2, p + phi*w3
 //   with w2 = w + phi*A1/2, w3 = w + phi*A2/2.
 // The phase integrand is n - 1 with n = sqrt(1 - (omega_pe/omega)^2) from the
 // interpolated density (src/legacy/full_solver.py:271-274, :341-347).
-template <class P, bool CACHE, bool IB>
+template <class P, int IB, bool SMALLX, bool CLAMP>
 __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, CellCache<P>& cc, typename P::R phi) {
     using R = typename P::R;
     const R two = R(2);
     const R hphi = R(0.5) * phi, phi6 = phi * R(1.0 / 6.0), phi2_6 = phi * phi6;
     const R S0 = (R)a.S[0], S1 = (R)a.S[1], S2 = (R)a.S[2];
     const R ope2 = (R)a.ope2;
-    R pe[3], we[3], sA[3], sW[3], w3[3], p3[3];
+    R ph[3], pl[3], we[3], sA[3], sW[3], w3[3], st[3];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
-        pe[x] = r.p[x].val();
+        ph[x] = r.p[x].hi();
+        pl[x] = r.p[x].lo();
         we[x] = r.w[x].val();
     }
     Sample<P> s;
     // stage 1 at p
-    sample_c<P, CACHE, IB>(a, pe[0], pe[1], pe[2], s, cc);
-    R g = P::n_minus_1(ope2 * s.q);
+    sample_c<P, IB, CLAMP>(a, ph, pl, s, cc);
+    R g = nm1<P, SMALLX>(ope2 * s.q);
     R kq = s.k;
     sA[0] = S0 * s.g0; sA[1] = S1 * s.g1; sA[2] = S2 * s.g2;
+    // stage 2 at p + phi*w/2
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         sW[x] = sA[x];
-        p3[x] = pe[x] + hphi * (we[x] + hphi * sA[x]);   // p + phi*w2/2
+        st[x] = pl[x] + hphi * we[x];
     }
-    // stage 2 at p + phi*w/2
-    sample_c<P, CACHE, IB>(a, pe[0] + hphi * we[0], pe[1] + hphi * we[1], pe[2] + hphi * we[2], s, cc);
+    sample_c<P, IB, CLAMP>(a, ph, st, s, cc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + hphi * (we[x] + hphi * sA[x]);   // p + phi*w2/2
     {
         const R A[3] = {S0 * s.g0, S1 * s.g1, S2 * s.g2};
 #pragma unroll
@@ -228,24 +280,25 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, CellCach
             sW[x] += two * A[x];
         }
     }
-    g += two * P::n_minus_1(ope2 * s.q);
+    g += two * nm1<P, SMALLX>(ope2 * s.q);
     kq += two * s.k;
     // stage 3 at p + phi*w2/2
-    sample_c<P, CACHE, IB>(a, p3[0], p3[1], p3[2], s, cc);
+    sample_c<P, IB, CLAMP>(a, ph, st, s, cc);
     {
         const R A[3] = {S0 * s.g0, S1 * s.g1, S2 * s.g2};
 #pragma unroll
         for (int x = 0; x < 3; ++x) {
             sA[x] += A[x];
             sW[x] += two * A[x];
+            st[x] = pl[x] + phi * w3[x];
         }
     }
-    g += two * P::n_minus_1(ope2 * s.q);
+    g += two * nm1<P, SMALLX>(ope2 * s.q);
     kq += two * s.k;
     // stage 4 at p + phi*w3
-    sample_c<P, CACHE, IB>(a, pe[0] + phi * w3[0], pe[1] + phi * w3[1], pe[2] + phi * w3[2], s, cc);
+    sample_c<P, IB, CLAMP>(a, ph, st, s, cc);
     sW[0] += S0 * s.g0; sW[1] += S1 * s.g1; sW[2] += S2 * s.g2;
-    g += P::n_minus_1(ope2 * s.q);
+    g += nm1<P, SMALLX>(ope2 * s.q);
     kq += s.k;
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
@@ -254,16 +307,18 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, CellCach
         r.w[x].add(phi6 * sW[x]);
     }
     r.ph += (double)(phi * g);
-    if constexpr (IB) r.tau.add(phi * kq);
+    if constexpr (IB != IB_OFF) r.tau.add(phi * kq);
 }
 
-// Fraction of the next step after which a ray inside the grid reaches a grid
-// face along its straight-line prediction p + w; 1 if it stays inside. The
-// RHS is discontinuous at the faces (fill 0 outside), so the step is cut there.
+// Kind of the next step of a ray: 0 plain step of a ray inside the grid whose
+// prediction stays more than kFaceMargin inside; 1 full step sampled with
+// clamped stage points (its prediction ends within kFaceMargin of a face);
+// 2 step cut at the face its prediction crosses, length phi, after which the
+// ray leaves; 3 plain step of a ray outside the grid (zero RHS).
 template <class P>
-__device__ __forceinline__ typename P::R exit_fraction(const TraceArgs& a, const Ray<P>& r) {
+__device__ __forceinline__ int step_kind(const TraceArgs& a, const Ray<P>& r, typename P::R& phi) {
     using R = typename P::R;
-    R phi = R(1);
+    const R margin = R(kFaceMargin);
     R p[3], w[3];
     bool in = true;
 #pragma unroll
@@ -272,16 +327,25 @@ __device__ __forceinline__ typename P::R exit_fraction(const TraceArgs& a, const
         w[x] = r.w[x].val();
         in = in & (p[x] >= R(0)) & (p[x] <= lim_of<R>(a.geo, x));
     }
-    if (in) {
+    phi = R(1);
+    if (!in) return 3;
+    bool near = false;
 #pragma unroll
-        for (int x = 0; x < 3; ++x) {
-            const R pn = p[x] + w[x];
-            const R lim = lim_of<R>(a.geo, x);
-            if (pn > lim) phi = fmin(phi, (lim - p[x]) / w[x]);
-            if (pn < R(0)) phi = fmin(phi, -p[x] / w[x]);
+    for (int x = 0; x < 3; ++x) {
+        const R pn = p[x] + w[x];
+        const R lim = lim_of<R>(a.geo, x);
+        if (pn > lim - margin) {
+            near = true;
+            // distance to the face from the compensated position
+            if (pn > lim) phi = fmin(phi, ((lim - r.p[x].hi()) - r.p[x].lo()) / w[x]);
+        }
+        if (pn < margin) {
+            near = true;
+            if (pn < R(0)) phi = fmin(phi, (-r.p[x].hi() - r.p[x].lo()) / w[x]);
         }
     }
-    return fmax(phi, R(0));
+    phi = fmax(phi, R(0));
+    return phi < R(1) ? 2 : (near ? 1 : 0);
 }
 
 template <class P>
@@ -314,7 +378,7 @@ __device__ __forceinline__ bool ray_gone(const TraceArgs& a, const Ray<P>& r) {
 // `drift` unit steps before the save time (drift > 0 only for rays that have
 // left the grid for good, whose path is a straight line).
 template <class R>
-__device__ __noinline__ void emit_save(const TraceArgs& a, unsigned id, int j, double drift,
+__device__ __forceinline__ void emit_save(const TraceArgs& a, unsigned id, int j, double drift,
                                        double p0, double p1, double p2, double w0, double w1,
                                        double w2, double ph, double tau) {
     double x[3], v[3];
@@ -370,9 +434,12 @@ __device__ __forceinline__ void finish_ray(const TraceArgs& a, const Ray<P>& r, 
 }
 
 // Saves due at the current step, then the end / exit checks. Returns true
-// while the ray still needs steps.
+// while the ray still needs steps. `check_gone` is false after a plain step
+// taken from inside the grid with its prediction more than kFaceMargin inside
+// (the ray cannot have left); the outside test is skipped then.
 template <class P>
-__device__ __forceinline__ bool settle(const TraceArgs& a, Ray<P>& r, unsigned long long& my_steps) {
+__device__ __forceinline__ bool settle(const TraceArgs& a, Ray<P>& r, unsigned long long& my_steps,
+                                      bool check_gone = true) {
     while (r.save_j < a.n_saves && r.next_save == r.step) {
         emit<P>(a, r, r.lag);
         ++r.save_j;
@@ -383,7 +450,7 @@ __device__ __forceinline__ bool settle(const TraceArgs& a, Ray<P>& r, unsigned l
                       my_steps);
         return false;
     }
-    if (r.exited || ray_gone<P>(a, r)) {
+    if (r.exited || (check_gone && ray_gone<P>(a, r))) {
         while (r.save_j < a.n_saves) {
             emit<P>(a, r, (double)(r.next_save - r.step) + r.lag);
             ++r.save_j;
@@ -440,8 +507,9 @@ __device__ __forceinline__ void tile_sort(unsigned* key, unsigned* id) {
     }
 }
 
-template <class P, bool CACHE, bool IB>
-__global__ void __launch_bounds__(kTraceThreads, 2) trace_kernel(const __grid_constant__ TraceArgs a) {
+template <class P, int IB, bool SMALLX>
+__global__ void __launch_bounds__(kThreads, SLOTH_TRACE_MIN_BLOCKS)
+trace_kernel(const __grid_constant__ TraceArgs a) {
     __shared__ unsigned s_key[kTile];
     __shared__ unsigned s_id[kTile];
     __shared__ int s_tile, s_head;
@@ -496,14 +564,19 @@ __global__ void __launch_bounds__(kTraceThreads, 2) trace_kernel(const __grid_co
                 continue;
             }
             if (active) {
-                const typename P::R phi = exit_fraction<P>(a, r);
-                rk4_step<P, CACHE, IB>(a, r, cc, phi);
-                ++r.step;
-                if (phi < typename P::R(1)) {
-                    r.exited = true;
-                    r.lag = 1.0 - (double)phi;
+                typename P::R phi;
+                const int kind = step_kind<P>(a, r, phi);
+                if (kind == 0 || kind == 3) {
+                    rk4_step<P, IB, SMALLX, false>(a, r, cc, typename P::R(1));
+                } else {
+                    rk4_step<P, IB, SMALLX, true>(a, r, cc, phi);
+                    if (kind == 2) {
+                        r.exited = true;
+                        r.lag = 1.0 - (double)phi;
+                    }
                 }
-                active = settle<P>(a, r, my_steps);
+                ++r.step;
+                active = settle<P>(a, r, my_steps, kind != 0);
             }
         }
         __syncthreads();
@@ -623,18 +696,24 @@ static int bucket_bits_for(long long n) {
     return bits;
 }
 
-template <class P, bool CACHE, bool IB>
-static int occupancy_blocks() {
+template <class P, int IB, bool SMALLX>
+static int launch_trace(const TraceArgs& ta, int sms, cudaStream_t s) {
     static int cached[64] = {0};
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return 1;
-    if (dev >= 0 && dev < 64 && cached[dev] > 0) return cached[dev];
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, trace_kernel<P, CACHE, IB>, kTraceThreads, 0) !=
-            cudaSuccess || b < 1)
-        b = 1;
-    if (dev >= 0 && dev < 64) cached[dev] = b;
-    return b;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e);
+    int per_sm = (dev >= 0 && dev < 64) ? cached[dev] : 0;
+    if (per_sm <= 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel<P, IB, SMALLX>, kThreads, 0) !=
+                cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        if (dev >= 0 && dev < 64) cached[dev] = per_sm;
+    }
+    long long blocks = (long long)sms * per_sm;
+    if (blocks > ta.n_tiles) blocks = ta.n_tiles;
+    trace_kernel<P, IB, SMALLX><<<(int)blocks, kThreads, 0, s>>>(ta);
+    note_launch();
+    return cuda_status(cudaGetLastError());
 }
 
 template <class P>
@@ -655,6 +734,7 @@ static int trace_impl(const SlothGridDesc* g, const void* grid, const SlothTrace
     if (last > 2000000000LL) return SLOTH_ERR_TOO_LARGE;
     if (p->inv_brems && !(p->kappa_q2 >= 0.0)) return SLOTH_ERR_INVALID_ARGUMENT;
     if (p->project_to_plane && !std::isfinite(p->plane)) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (!std::isfinite(p->q_max)) return SLOTH_ERR_INVALID_ARGUMENT;
     if (n == 0) {
         if (out->total_steps) {
             cudaError_t e = cudaMemsetAsync(out->total_steps, 0, sizeof(unsigned long long), (cudaStream_t)stream);
@@ -719,6 +799,8 @@ static int trace_impl(const SlothGridDesc* g, const void* grid, const SlothTrace
     note_launch();
     scatter_kernel<<<kb, 256, 0, s>>>(keys, n, 30 - bbits, hist, perm, skeys);
     note_launch();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e);
 
     TraceArgs ta;
     ta.geo = make_geo(g);
@@ -750,7 +832,6 @@ static int trace_impl(const SlothGridDesc* g, const void* grid, const SlothTrace
     ta.t1 = t1;
     ta.t2 = t2;
     ta.project = p->project_to_plane ? 1 : 0;
-    ta.inv_brems = p->inv_brems ? 1 : 0;
     ta.jones = out->jones;
     ta.state = out->state;
     ta.phase = out->phase;
@@ -759,28 +840,29 @@ static int trace_impl(const SlothGridDesc* g, const void* grid, const SlothTrace
     ta.steps = out->steps;
     ta.total_steps = out->total_steps;
 
-    constexpr bool kCache = false;
+    // q_max > 0 bounds ne/nc over the grid (the caller's promise): it selects
+    // the sub-critical kappa path and the series form of n - 1.
+    const double xmax = p->q_max > 0.0 ? p->q_max * p->ope_ratio2 : 1e300;
+    const bool smallx = xmax <= kSmallX;
+    const int ib = !p->inv_brems ? IB_OFF : (xmax <= 1.0 ? IB_SUBCRITICAL : IB_GENERAL);
+
     if (out->trace_event_begin) {
         e = cudaEventRecord((cudaEvent_t)out->trace_event_begin, s);
         if (e != cudaSuccess) return cuda_status(e);
     }
-    if (ta.inv_brems) {
-        const int per_sm = occupancy_blocks<P, kCache, true>();
-        const long long blocks = (long long)sms * per_sm < ta.n_tiles ? (long long)sms * per_sm : ta.n_tiles;
-        trace_kernel<P, kCache, true><<<(int)blocks, kTraceThreads, 0, s>>>(ta);
-    } else {
-        const int per_sm = occupancy_blocks<P, kCache, false>();
-        const long long blocks = (long long)sms * per_sm < ta.n_tiles ? (long long)sms * per_sm : ta.n_tiles;
-        trace_kernel<P, kCache, false><<<(int)blocks, kTraceThreads, 0, s>>>(ta);
-    }
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e);
+    if (ib == IB_OFF)
+        rc = smallx ? launch_trace<P, IB_OFF, true>(ta, sms, s) : launch_trace<P, IB_OFF, false>(ta, sms, s);
+    else if (ib == IB_SUBCRITICAL)
+        rc = smallx ? launch_trace<P, IB_SUBCRITICAL, true>(ta, sms, s)
+                    : launch_trace<P, IB_SUBCRITICAL, false>(ta, sms, s);
+    else
+        rc = launch_trace<P, IB_GENERAL, false>(ta, sms, s);
+    if (rc) return rc;
     if (out->trace_event_end) {
         e = cudaEventRecord((cudaEvent_t)out->trace_event_end, s);
         if (e != cudaSuccess) return cuda_status(e);
     }
-    note_launch();
-    return cuda_status(cudaGetLastError());
+    return SLOTH_OK;
 }
 
 }  // namespace sloth

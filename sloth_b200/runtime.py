@@ -61,6 +61,7 @@ class DeviceGrid:
     n: tuple
     origin: tuple
     spacing: tuple
+    q_max: float = 0.0         # max of the q channel (ne/nc) over the grid; 0 = unknown
 
     @property
     def nc(self) -> float:
@@ -105,7 +106,9 @@ def pack_grid(ne, origin, spacing, omega, *, precision="f32", device=None, strea
     scale = 1.0 / physics.critical_density(omega) if ne_scale is None else float(ne_scale)
     capi.check(fn(desc, capi.ptr(ne), int(ne.dtype == torch.float64), scale, capi.ptr(out), _stream_ptr(stream)),
                "sloth_grid_pack")
-    return DeviceGrid(out, desc, precision, float(omega), n, tuple(map(float, origin)), tuple(map(float, spacing)))
+    q_max = float(ne.max()) * scale if ne.numel() else 0.0
+    return DeviceGrid(out, desc, precision, float(omega), n, tuple(map(float, origin)), tuple(map(float, spacing)),
+                      q_max=max(q_max, 0.0) * (1.0 + 1e-6))
 
 
 def sample(grid: DeviceGrid, points, *, stream=None) -> torch.Tensor:
@@ -227,6 +230,7 @@ def trace(grid: DeviceGrid, rays: torch.Tensor, sched: Schedule, *, axis=2, proj
         p.kappa_q2, p.coulomb_log_w, p.ope_ratio2 = kq2, clw, ope2
     else:
         p.kappa_q2, p.coulomb_log_w, p.ope_ratio2 = 0.0, 2.0, physics.ope_ratio2(grid.omega)
+    p.q_max = float(grid.q_max)
     out = capi.SlothTraceOutputs()
     out.jones = capi.ptr(jones)
     out.state = capi.ptr(state)

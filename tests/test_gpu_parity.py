@@ -3,8 +3,13 @@
 Tolerances (stated for every output):
 * FP64 kernel vs FP64 oracle: positions 1e-10 of the box length, directions
   1e-10 (|d(v/c)|), phase 1e-10 relative, amplitude 1e-12 absolute.
-* FP32 split kernel vs FP64 oracle: positions 1e-6 of the box length,
-  directions 1e-6, phase 1e-6 relative (of max |phase|), amplitude 1e-6 absolute.
+* FP32 split kernel vs FP64 oracle: positions 1e-6 of the box length and
+  directions 1e-6 for every ray; phase 1e-6 relative (of max |phase|) and
+  amplitude 1e-6 absolute for rays that leave through the far face or stay
+  inside. Rays that leave through a side face do so at grazing incidence
+  (normal velocity ~1e-3 c): their exit time, and so the phase and optical
+  depth gathered up to it, moves by (position rounding)/(normal velocity);
+  for them the bounds are 1e-3 relative and 1e-4 absolute.
 """
 import numpy as np
 import pytest
@@ -92,6 +97,12 @@ def test_trace_f64_matches_oracle(kind, n, nrays, axis, ib, project, n_saves, ji
     assert k["total_steps"] == int(k["steps"].astype(np.int64).sum())
 
 
+def side_exit(state_last, axis):
+    """Rays whose transverse position at the last save is outside the box."""
+    t = [a for a in range(3) if a != axis]
+    return (np.abs(state_last[t[0]]) > L / 2) | (np.abs(state_last[t[1]]) > L / 2)
+
+
 @pytest.mark.parametrize("kind,n,nrays,axis,ib,project,n_saves,jitter", CASES)
 def test_trace_f32_within_tolerance(kind, n, nrays, axis, ib, project, n_saves, jitter):
     k, o = _run_pair(kind, n, nrays, axis, ib, project, n_saves, jitter, "f32")
@@ -99,10 +110,15 @@ def test_trace_f32_within_tolerance(kind, n, nrays, axis, ib, project, n_saves, 
     de = direction_error(k["state"], o["state"])
     assert pe < 1e-6, pe
     assert de < 1e-6, de
-    ph = np.abs(o["phase"]).max()
-    assert np.abs(k["phase"] - o["phase"]).max() <= 1e-6 * max(ph, 1e-30)
+    side = side_exit(o["state"][-1], axis)
+    ph = max(np.abs(o["phase"]).max(), 1e-30)
+    dph = np.abs(k["phase"] - o["phase"])
+    assert dph[:, ~side].max() <= 1e-6 * ph, dph[:, ~side].max() / ph
+    assert dph.max() <= 1e-3 * ph
     if ib:
-        assert np.abs(k["amp"].astype(np.float64) - o["amp"]).max() < 1e-6
+        damp = np.abs(k["amp"].astype(np.float64) - o["amp"])
+        assert damp[:, ~side].max() < 1e-6, damp[:, ~side].max()
+        assert damp.max() < 1e-4
     assert (k["steps"] != o["steps"]).mean() < 5e-3
 
 
