@@ -156,6 +156,28 @@ int sloth_trace_f64(const SlothGridDesc* g, const void* grid, const SlothTracePa
                     const double* rays, int64_t n, const SlothTraceOutputs* out,
                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- allocation-free FP32 tracer ------------------------------------------
+ * No counterpart in the reference. Some callers cannot allocate device
+ * memory: an XLA FFI handler inside a JAX program (the reference's own
+ * runtime) is handed only its operand and result buffers, and XLA has
+ * already reserved most of the GPU for itself; an embedded or real-time host
+ * may forbid device allocation after start-up. sloth_trace_f32 needs a caller
+ * workspace; this variant takes the same inputs and outputs and keeps its
+ * scratch in a fixed device array inside the library instead, so it
+ * allocates nothing (no cudaMalloc, no cudaFree, no allocating library call).
+ * Limits and rules:
+ *   - n <= SLOTH_NOALLOC_MAX_RAYS, else SLOTH_ERR_TOO_LARGE;
+ *   - the array (about 13.6 MB) is held on every GPU that loads the library
+ *     until the process exits;
+ *   - the first call on each device looks up the array's device address with
+ *     cudaGetSymbolAddress; make that first call before any stream capture;
+ *   - every call shares the array, so calls that overlap on the GPU (other
+ *     streams, other host threads) race: serialise them.
+ * Results equal sloth_trace_f32's for the same inputs. */
+#define SLOTH_NOALLOC_MAX_RAYS (1 << 20)
+int sloth_trace_f32_noalloc(const SlothGridDesc* g, const void* grid, const SlothTraceParams* p,
+                            const float* rays, int64_t n, const SlothTraceOutputs* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,7 @@ SLOTH_RAY_INSIDE_AT_END = 1
 SLOTH_RAY_NONFINITE = 2
 
 SLOTH_MAX_SAVES = 4096
+SLOTH_NOALLOC_MAX_RAYS = 1 << 20
 
 
 class SlothExtensionMissing(ImportError):
@@ -85,6 +86,8 @@ _SIGNATURES = {
                                 c_int64, POINTER(SlothTraceOutputs), c_void_p, c_size_t, c_void_p]),
     "sloth_trace_f64": (c_int, [POINTER(SlothGridDesc), c_void_p, POINTER(SlothTraceParams), c_void_p,
                                 c_int64, POINTER(SlothTraceOutputs), c_void_p, c_size_t, c_void_p]),
+    "sloth_trace_f32_noalloc": (c_int, [POINTER(SlothGridDesc), c_void_p, POINTER(SlothTraceParams), c_void_p,
+                                        c_int64, POINTER(SlothTraceOutputs), c_void_p]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGNATURES)

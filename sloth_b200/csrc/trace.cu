@@ -30,6 +30,7 @@
 //                      finished are refilled from the tile with one warp
 //                      ballot + one shared-memory atomic per refill.
 #include <cmath>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -682,8 +683,8 @@ __global__ void __launch_bounds__(256) scatter_kernel(const unsigned* __restrict
 // ---------------------------------------------------------------------------
 static size_t align256(size_t x) { return (x + 255u) & ~(size_t)255u; }
 
-static const size_t kHeaderBytes = 256;
-static const size_t kHistBytes = (size_t)4 << kMaxBucketBits;
+constexpr size_t kHeaderBytes = 256;
+constexpr size_t kHistBytes = (size_t)4 << kMaxBucketBits;
 
 static size_t workspace_bytes(long long n) {
     const size_t a = align256((size_t)(n > 0 ? n : 1) * 4u);
@@ -865,11 +866,56 @@ static int trace_impl(const SlothGridDesc* g, const void* grid, const SlothTrace
     return SLOTH_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the FP32 tracer: its scratch (tile counter,
+// bucket histogram, keys, permutation) lives in one file-scope device array
+// sized for SLOTH_NOALLOC_MAX_RAYS rays, so the caller passes only inputs and
+// outputs and nothing here allocates. Host code cannot use the array's name
+// as a device address; each device's address is looked up once, on that
+// device's first call, with cudaGetSymbolAddress. All calls share the array,
+// which keeps the previous call's contents (the tracer zeroes the parts that
+// must start at zero), so calls that overlap on the GPU race.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = kHeaderBytes + kHistBytes + 3 * (size_t)4 * SLOTH_NOALLOC_MAX_RAYS;
+static_assert(kNoAllocScratchBytes % 256 == 0, "scratch sections must stay 256-byte aligned");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_addr[64] = {nullptr};
+
+static int noalloc_scratch(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (dev < 0 || dev >= 64) return SLOTH_ERR_UNSUPPORTED_DEVICE;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_addr[dev] == nullptr) {
+        void* addr = nullptr;
+        e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_status(e);
+        g_noalloc_addr[dev] = addr;
+    }
+    *out = g_noalloc_addr[dev];
+    return SLOTH_OK;
+}
+
 }  // namespace sloth
 
 extern "C" {
 
 size_t sloth_trace_workspace_bytes(int64_t n_rays) { return sloth::workspace_bytes(n_rays); }
+
+int sloth_trace_f32_noalloc(const SlothGridDesc* g, const void* grid, const SlothTraceParams* p,
+                            const float* rays, int64_t n, const SlothTraceOutputs* out, void* stream) {
+    if (n < 0) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (n > (int64_t)SLOTH_NOALLOC_MAX_RAYS) return SLOTH_ERR_TOO_LARGE;
+    void* scratch = nullptr;
+    const int rc = sloth::noalloc_scratch(&scratch);
+    if (rc) return rc;
+    return sloth::trace_impl<sloth::PolF32>(g, grid, p, rays, n, out, scratch, sloth::kNoAllocScratchBytes,
+                                            stream);
+}
 
 int sloth_trace_f32(const SlothGridDesc* g, const void* grid, const SlothTraceParams* p, const float* rays,
                     int64_t n, const SlothTraceOutputs* out, void* workspace, size_t workspace_bytes,
