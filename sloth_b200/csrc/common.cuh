@@ -45,19 +45,20 @@ __host__ __device__ inline unsigned morton_key(unsigned c1, unsigned c2, unsigne
 // Precision policies.
 // ---------------------------------------------------------------------------
 
-// FP32 sum carried with a Neumaier (Kahan-Babuska) compensation term: the
-// value is s + c. Used for positions, velocities and the optical depth so that
-// ~10^3 small increments onto an O(1..10^3) running value keep FP64-like
-// accuracy without FP64 arithmetic.
+// FP32 sum carried with a Kahan compensation term: the value is s + c, c
+// holding the rounding error lost by the running sum. Used for positions,
+// velocities and the optical depth so that ~10^3 small increments onto an
+// O(1..10^3) running value keep FP64-like accuracy without FP64 arithmetic.
 struct AccF {
     float s, c;
     __device__ __forceinline__ void set(double v) {
         s = (float)v;
         c = (float)(v - (double)s);
     }
-    __device__ __forceinline__ void add(float y) {
+    __device__ __forceinline__ void add(float x) {
+        const float y = x + c;
         const float t = s + y;
-        c += (fabsf(s) >= fabsf(y)) ? ((s - t) + y) : ((y - t) + s);
+        c = y - (t - s);
         s = t;
     }
     __device__ __forceinline__ float val() const { return s + c; }
@@ -85,6 +86,12 @@ struct Vox4D { double x, y, z, w; };
 #ifndef SLOTH_CELL_CACHE_F64
 #define SLOTH_CELL_CACHE_F64 1
 #endif
+#ifndef SLOTH_CELL_POLY_F32
+#define SLOTH_CELL_POLY_F32 1
+#endif
+#ifndef SLOTH_CELL_POLY_F64
+#define SLOTH_CELL_POLY_F64 0
+#endif
 
 struct PolF32 {
     using R = float;
@@ -92,6 +99,9 @@ struct PolF32 {
     using Acc = AccF;
     // keep the last cell's 8 corners in registers across stages and steps
     static constexpr bool cell_cache = SLOTH_CELL_CACHE_F32 != 0;
+    // keep the cached cell as trilinear polynomial coefficients (7 FMAs per
+    // channel per sample instead of 8 products and an 8-term sum)
+    static constexpr bool cell_poly = SLOTH_CELL_POLY_F32 != 0;
     __device__ __forceinline__ static V load(const void* g, unsigned i) {
         const float4 v = __ldg(reinterpret_cast<const float4*>(g) + i);
         return V{v.x, v.y, v.z, v.w};
@@ -111,6 +121,7 @@ struct PolF64 {
     using V = Vox4D;
     using Acc = AccD;
     static constexpr bool cell_cache = SLOTH_CELL_CACHE_F64 != 0;
+    static constexpr bool cell_poly = SLOTH_CELL_POLY_F64 != 0;
     __device__ __forceinline__ static V load(const void* g, unsigned i) {
         const double2* p = reinterpret_cast<const double2*>(g) + 2u * (size_t)i;
         const double2 a = __ldg(p), b = __ldg(p + 1);

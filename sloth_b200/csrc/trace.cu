@@ -31,6 +31,7 @@
 //                      ballot + one shared-memory atomic per refill.
 #include <cmath>
 #include <mutex>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -110,6 +111,38 @@ struct Sample {
     typename P::R q, g0, g1, g2, k;
 };
 
+// A cached cell as trilinear polynomials in the in-cell coordinates
+// (fx, fy, fz): per channel T = a + bx fx + by fy + bz fz + cxy fx fy +
+// cxz fx fz + cyz fy fz + cxyz fx fy fz, channels q, dq/du, dq/dv, dq/dw and
+// (when NK = 5) the inverse-bremsstrahlung corner rate.
+template <class P, int NK>
+struct CellPoly {
+    unsigned base;
+    typename P::R t[NK][8];
+};
+
+template <class R>
+__device__ __forceinline__ void poly_coeffs(R (&t)[8], R v0, R v1, R v2, R v3, R v4, R v5, R v6, R v7) {
+    // corner index = 4*dx + 2*dy + dz
+    const R bz = v1 - v0, by = v2 - v0, bx = v4 - v0;
+    const R dyz = v3 - v2, dxz = v5 - v4, dxy = v6 - v4;
+    t[0] = v0;
+    t[1] = bx;
+    t[2] = by;
+    t[3] = bz;
+    t[4] = dxy - by;                       // cxy
+    t[5] = dxz - bz;                       // cxz
+    t[6] = dyz - bz;                       // cyz
+    t[7] = ((v7 - v6) - dxz) - (dyz - bz); // cxyz
+}
+
+template <class R>
+__device__ __forceinline__ R poly_eval(const R (&t)[8], R fx, R fy, R fz) {
+    const R cz = (t[3] + fx * t[5]) + fy * (t[6] + fx * t[7]);   // coefficient of fz
+    const R cy = t[2] + fx * t[4];                               // coefficient of fy (without fz)
+    return ((t[0] + fx * t[1]) + fy * cy) + fz * cz;
+}
+
 // n - 1 for n = sqrt(1 - x), x = (omega_pe/omega)^2. SMALLX (FP32 only, used
 // when x <= kSmallX over the whole grid) takes the binomial series
 // -(x/2 + x^2/8 + x^3/16 + 5x^4/128 + 7x^5/256), whose first omitted term is
@@ -148,9 +181,9 @@ __device__ __forceinline__ typename P::R corner_kappa(const TraceArgs& a, typena
 // rounded sum; the weights from (hi - i) + lo, which resolves the position
 // inside the cell to FP32 relative precision rather than FP32 precision of
 // the absolute position. CLAMP moves the point into the grid first.
-template <class P, int IB, bool CLAMP>
+template <class P, int IB, bool CLAMP, class Cache>
 __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R (&hi)[3],
-                                         const typename P::R (&lo)[3], Sample<P>& out, CellCache<P>& cc) {
+                                         const typename P::R (&lo)[3], Sample<P>& out, Cache& cc) {
     using R = typename P::R;
     using V = typename P::V;
     const GridGeo& g = a.geo;
@@ -180,58 +213,91 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
     const int iz = min((int)p[2], g.n[2] - 2);
     const R fx = (h[0] - (R)ix) + l[0], fy = (h[1] - (R)iy) + l[1], fz = (h[2] - (R)iz) + l[2];
     const unsigned b = (unsigned)ix * g.sx + (unsigned)iy * g.sy + (unsigned)iz;
-    V c[8];
-    if constexpr (P::cell_cache) {
+    if constexpr (P::cell_poly) {
         if (b != cc.base) {
             cc.base = b;
-            cc.c[0] = P::load(a.grid, b);
-            cc.c[1] = P::load(a.grid, b + 1u);
-            cc.c[2] = P::load(a.grid, b + g.sy);
-            cc.c[3] = P::load(a.grid, b + g.sy + 1u);
-            cc.c[4] = P::load(a.grid, b + g.sx);
-            cc.c[5] = P::load(a.grid, b + g.sx + 1u);
-            cc.c[6] = P::load(a.grid, b + g.sx + g.sy);
-            cc.c[7] = P::load(a.grid, b + g.sx + g.sy + 1u);
+            const V v0 = P::load(a.grid, b), v1 = P::load(a.grid, b + 1u);
+            const V v2 = P::load(a.grid, b + g.sy), v3 = P::load(a.grid, b + g.sy + 1u);
+            const V v4 = P::load(a.grid, b + g.sx), v5 = P::load(a.grid, b + g.sx + 1u);
+            const V v6 = P::load(a.grid, b + g.sx + g.sy), v7 = P::load(a.grid, b + g.sx + g.sy + 1u);
+            poly_coeffs<R>(cc.t[0], v0.x, v1.x, v2.x, v3.x, v4.x, v5.x, v6.x, v7.x);
+            poly_coeffs<R>(cc.t[1], v0.y, v1.y, v2.y, v3.y, v4.y, v5.y, v6.y, v7.y);
+            poly_coeffs<R>(cc.t[2], v0.z, v1.z, v2.z, v3.z, v4.z, v5.z, v6.z, v7.z);
+            poly_coeffs<R>(cc.t[3], v0.w, v1.w, v2.w, v3.w, v4.w, v5.w, v6.w, v7.w);
+            if constexpr (IB == IB_SUBCRITICAL) {
+                poly_coeffs<R>(cc.t[4 % (IB ? 5 : 4)], v0.x * v0.x, v1.x * v1.x, v2.x * v2.x, v3.x * v3.x,
+                               v4.x * v4.x, v5.x * v5.x, v6.x * v6.x, v7.x * v7.x);
+            } else if constexpr (IB == IB_GENERAL) {
+                poly_coeffs<R>(cc.t[4 % (IB ? 5 : 4)], corner_kappa<P>(a, v0.x), corner_kappa<P>(a, v1.x),
+                               corner_kappa<P>(a, v2.x), corner_kappa<P>(a, v3.x), corner_kappa<P>(a, v4.x),
+                               corner_kappa<P>(a, v5.x), corner_kappa<P>(a, v6.x), corner_kappa<P>(a, v7.x));
+            }
         }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) c[i] = cc.c[i];
+        out.q = poly_eval<R>(cc.t[0], fx, fy, fz);
+        out.g0 = poly_eval<R>(cc.t[1], fx, fy, fz);
+        out.g1 = poly_eval<R>(cc.t[2], fx, fy, fz);
+        out.g2 = poly_eval<R>(cc.t[3], fx, fy, fz);
+        if constexpr (IB == IB_SUBCRITICAL) {
+            out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz) * (R)a.cl_lo;
+        } else if constexpr (IB == IB_GENERAL) {
+            out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz);
+        } else {
+            out.k = R(0);
+        }
     } else {
-        c[0] = P::load(a.grid, b);
-        c[1] = P::load(a.grid, b + 1u);
-        c[2] = P::load(a.grid, b + g.sy);
-        c[3] = P::load(a.grid, b + g.sy + 1u);
-        c[4] = P::load(a.grid, b + g.sx);
-        c[5] = P::load(a.grid, b + g.sx + 1u);
-        c[6] = P::load(a.grid, b + g.sx + g.sy);
-        c[7] = P::load(a.grid, b + g.sx + g.sy + 1u);
-    }
-    const R ex = R(1) - fx, ey = R(1) - fy, ez = R(1) - fz;
-    const R w00 = ex * ey, w01 = ex * fy, w10 = fx * ey, w11 = fx * fy;
-    const R w[8] = {w00 * ez, w00 * fz, w01 * ez, w01 * fz, w10 * ez, w10 * fz, w11 * ez, w11 * fz};
-    R q = R(0), g0 = R(0), g1 = R(0), g2 = R(0);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        q += c[i].x * w[i];
-        g0 += c[i].y * w[i];
-        g1 += c[i].z * w[i];
-        g2 += c[i].w * w[i];
-    }
-    out.q = q;
-    out.g0 = g0;
-    out.g1 = g1;
-    out.g2 = g2;
-    if constexpr (IB == IB_SUBCRITICAL) {
-        R k = R(0);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) k += w[i] * (c[i].x * c[i].x);
-        out.k = k * (R)a.cl_lo;
-    } else if constexpr (IB == IB_GENERAL) {
-        R k = R(0);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) k += w[i] * corner_kappa<P>(a, c[i].x);
-        out.k = k;
-    } else {
-        out.k = R(0);
+        V c[8];
+        if constexpr (P::cell_cache) {
+            if (b != cc.base) {
+                cc.base = b;
+                cc.c[0] = P::load(a.grid, b);
+                cc.c[1] = P::load(a.grid, b + 1u);
+                cc.c[2] = P::load(a.grid, b + g.sy);
+                cc.c[3] = P::load(a.grid, b + g.sy + 1u);
+                cc.c[4] = P::load(a.grid, b + g.sx);
+                cc.c[5] = P::load(a.grid, b + g.sx + 1u);
+                cc.c[6] = P::load(a.grid, b + g.sx + g.sy);
+                cc.c[7] = P::load(a.grid, b + g.sx + g.sy + 1u);
+            }
+    #pragma unroll
+            for (int i = 0; i < 8; ++i) c[i] = cc.c[i];
+        } else {
+            c[0] = P::load(a.grid, b);
+            c[1] = P::load(a.grid, b + 1u);
+            c[2] = P::load(a.grid, b + g.sy);
+            c[3] = P::load(a.grid, b + g.sy + 1u);
+            c[4] = P::load(a.grid, b + g.sx);
+            c[5] = P::load(a.grid, b + g.sx + 1u);
+            c[6] = P::load(a.grid, b + g.sx + g.sy);
+            c[7] = P::load(a.grid, b + g.sx + g.sy + 1u);
+        }
+        const R ex = R(1) - fx, ey = R(1) - fy, ez = R(1) - fz;
+        const R w00 = ex * ey, w01 = ex * fy, w10 = fx * ey, w11 = fx * fy;
+        const R w[8] = {w00 * ez, w00 * fz, w01 * ez, w01 * fz, w10 * ez, w10 * fz, w11 * ez, w11 * fz};
+        R q = R(0), g0 = R(0), g1 = R(0), g2 = R(0);
+    #pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            q += c[i].x * w[i];
+            g0 += c[i].y * w[i];
+            g1 += c[i].z * w[i];
+            g2 += c[i].w * w[i];
+        }
+        out.q = q;
+        out.g0 = g0;
+        out.g1 = g1;
+        out.g2 = g2;
+        if constexpr (IB == IB_SUBCRITICAL) {
+            R k = R(0);
+    #pragma unroll
+            for (int i = 0; i < 8; ++i) k += w[i] * (c[i].x * c[i].x);
+            out.k = k * (R)a.cl_lo;
+        } else if constexpr (IB == IB_GENERAL) {
+            R k = R(0);
+    #pragma unroll
+            for (int i = 0; i < 8; ++i) k += w[i] * corner_kappa<P>(a, c[i].x);
+            out.k = k;
+        } else {
+            out.k = R(0);
+        }
     }
 }
 
@@ -243,8 +309,8 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
 //   with w2 = w + phi*A1/2, w3 = w + phi*A2/2.
 // The phase integrand is n - 1 with n = sqrt(1 - (omega_pe/omega)^2) from the
 // interpolated density (src/legacy/full_solver.py:271-274, :341-347).
-template <class P, int IB, bool SMALLX, bool CLAMP>
-__device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, CellCache<P>& cc, typename P::R phi) {
+template <class P, int IB, bool SMALLX, bool CLAMP, class Cache>
+__device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
     using R = typename P::R;
     const R two = R(2);
     const R hphi = R(0.5) * phi, phi6 = phi * R(1.0 / 6.0), phi2_6 = phi * phi6;
@@ -520,7 +586,8 @@ trace_kernel(const __grid_constant__ TraceArgs a) {
     const unsigned lt_mask = (1u << lane) - 1u;
     unsigned long long my_steps = 0;
     if (threadIdx.x == 0) s_steps = 0;
-    CellCache<P> cc;
+    // register cache of the last cell: corners, or polynomial coefficients
+    typename std::conditional<P::cell_poly, CellPoly<P, (IB != IB_OFF) ? 5 : 4>, CellCache<P>>::type cc;
     cc.base = 0xffffffffu;
     for (;;) {
         if (threadIdx.x == 0) {
