@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -202,6 +204,40 @@ def run_reference(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# serving leg: 2000 requests, Poisson arrivals at 200/s, grids {64..384}^3
+# (sinusoid or Kolmogorov by a fair coin), lognormal ray counts (median 2e5,
+# sigma 1, clipped to [1e4, 4e6]), 120 GB admission budget
+# ---------------------------------------------------------------------------
+def run_serving(args):
+    import torch
+    from sloth_b200 import serving
+    reqs = serving.request_stream(args.serving_requests, rate=200.0, seed=args.seed)
+    fields = {}
+    for r in reqs:
+        k = serving.grid_key(r.kind, r.n, r.field_seed)
+        if k not in fields:
+            fields[k] = serving.field_for(r.kind, r.n, r.field_seed)
+    torch.cuda.synchronize()
+    out = {}
+    with serving.RayServer(120 << 30) as srv:
+        live = serving.replay(srv, reqs, fields=fields, realtime=True)
+    with serving.RayServer(120 << 30) as srv:
+        sat = serving.replay(srv, reqs, fields=fields, realtime=False)
+    out = {"requests": live["requests"], "rate_per_s": 200.0, "p50_ms": live["p50_ms"], "p99_ms": live["p99_ms"],
+           "mean_ms": live["mean_ms"], "ray_steps_per_s": live["ray_steps_per_s"], "ray_steps": live["ray_steps"],
+           "seconds": live["seconds"],
+           "saturated_ray_steps_per_s": sat["ray_steps_per_s"], "saturated_seconds": sat["seconds"],
+           "iterations": live["stats"]["iterations"], "grid_packs": live["stats"]["grid_packs"],
+           "budget_bytes": live["stats"]["budget_bytes"],
+           "stream": "2000 requests, Poisson 200/s, grids {64,128,192,256,384}^3 sinusoid|Kolmogorov, "
+                     "lognormal rays median 2e5 sigma 1 in [1e4, 4e6], 120 GB budget; latency = arrival to "
+                     "results in pinned host memory"}
+    del fields
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -364,6 +400,11 @@ def run_sloth(args):
                "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3,
                "path": "sloth_b200.core.propagator.solve (pinned host ne and rays, numpy outputs)"}
 
+    # ---- serving: the mixed request stream (p50/p99 latency) ----------------
+    serve = None
+    if not args.no_serving:
+        serve = run_serving(args)
+
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -399,6 +440,7 @@ def run_sloth(args):
             "clocks": clk.summary(),
             "fp64_port": fp64,
             "fp32_vs_fp64": acc,
+            "serving": serve,
         }
         if fp64:
             line["fp64_port"]["speedup_of_fp32"] = value / world / fp64["value"]

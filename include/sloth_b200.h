@@ -156,6 +156,70 @@ int sloth_trace_f64(const SlothGridDesc* g, const void* grid, const SlothTracePa
                     const double* rays, int64_t n, const SlothTraceOutputs* out,
                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- request server -------------------------------------------------------
+ * No counterpart in the reference (SLOTH traces one batch per call). Serves a
+ * stream of trace jobs of different grids and ray counts by continuous
+ * batching: one device arena of budget_bytes (allocated at create) holds the
+ * packed grids -- an LRU cache keyed by the caller's 64-bit grid key -- and
+ * each admitted job's rays, sort workspace and outputs. Jobs are admitted in
+ * submission order as memory and job-table slots free up. Every
+ * sloth_server_step() retires finished work, admits waiting jobs, and
+ * launches one iteration -- a captured CUDA graph running the FP32 tracer's
+ * persistent kernels over tiles handed out round-robin to all admitted jobs
+ * (quantum tiles per job per round, at most tiles_per_step tiles) -- with up
+ * to two iterations in flight. Results of a job do not depend on the other
+ * jobs in its iterations. Lifecycle of a job:
+ *   PENDING -> RUNNING (admitted) -> DONE -> fetch -> FETCHING -> FETCHED
+ * (memory released), or a negative SLOTH_ERR_* state if admission failed.
+ * The caller keeps `ne` (needed until the job is admitted, and only if the
+ * grid key is not resident) and `rays` valid until the job leaves PENDING.
+ * A handle may be used from several host threads (calls are serialised). */
+typedef struct SlothServer SlothServer;
+
+typedef struct SlothServerConfig {
+    size_t  budget_bytes;    /* device arena for grids and jobs (>= 16 MiB)      */
+    int32_t max_jobs;        /* jobs admitted at the same time (table slots)     */
+    int32_t tiles_per_step;  /* 1024-ray tiles per iteration                     */
+    int32_t quantum;         /* tiles per job per round-robin round              */
+    int32_t reserved;        /* must be 0                                        */
+} SlothServerConfig;
+
+typedef struct SlothServerStats {
+    size_t    budget_bytes, arena_used;
+    long long grids_resident, grid_packs, grid_evictions;
+    long long jobs_submitted, jobs_admitted, jobs_done, jobs_failed;
+    long long iterations, tiles, kernel_launches;
+} SlothServerStats;
+
+#define SLOTH_JOB_PENDING  0
+#define SLOTH_JOB_RUNNING  1
+#define SLOTH_JOB_DONE     2
+#define SLOTH_JOB_FETCHING 3
+#define SLOTH_JOB_FETCHED  4
+
+int sloth_server_create(const SlothServerConfig* cfg, SlothServer** out);
+int sloth_server_destroy(SlothServer* s);
+/* Queues a job. ne (device, float32 or float64 per ne_is_f64, m^-3) is packed
+ * when the job is admitted unless grid_key is resident (then ne may be NULL).
+ * rays: (6, n) float32, host memory (pinned) if rays_on_host, else device.
+ * p as for sloth_trace_f32 (its q_max selects the fast exact paths).
+ * SLOTH_ERR_TOO_LARGE if the job can never fit in the arena. */
+int sloth_server_submit(SlothServer* s, uint64_t grid_key, const SlothGridDesc* g, const void* ne,
+                        int ne_is_f64, const SlothTraceParams* p, const float* rays, int rays_on_host,
+                        int64_t n, int* job_id);
+/* One scheduling step; never blocks on the GPU. */
+int sloth_server_step(SlothServer* s, int* n_running, int* n_pending);
+int sloth_server_job_state(SlothServer* s, int job_id, int* state);
+/* Starts the download of a DONE job's outputs into dst (host or device
+ * pointers; NULL skips; element types as for sloth_trace_f32, no state);
+ * the job's memory is released once the copy has finished (FETCHED). */
+int sloth_server_fetch(SlothServer* s, int job_id, const SlothTraceOutputs* dst);
+/* Forgets a DONE or FETCHED job (a DONE job's memory is released unread). */
+int sloth_server_release(SlothServer* s, int job_id);
+int sloth_server_stats(SlothServer* s, SlothServerStats* st);
+/* Waits for all work the server has launched. */
+int sloth_server_sync(SlothServer* s);
+
 /* ---- allocation-free FP32 tracer ------------------------------------------
  * No counterpart in the reference. Some callers cannot allocate device
  * memory: an XLA FFI handler inside a JAX program (the reference's own

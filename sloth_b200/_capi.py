@@ -70,6 +70,22 @@ class SlothTraceOutputs(Structure):
                 ("total_steps", c_void_p), ("trace_event_begin", c_void_p), ("trace_event_end", c_void_p)]
 
 
+class SlothServerConfig(Structure):
+    _fields_ = [("budget_bytes", c_size_t), ("max_jobs", c_int32), ("tiles_per_step", c_int32),
+                ("quantum", c_int32), ("reserved", c_int32)]
+
+
+class SlothServerStats(Structure):
+    _fields_ = [("budget_bytes", c_size_t), ("arena_used", c_size_t), ("grids_resident", ctypes.c_longlong),
+                ("grid_packs", ctypes.c_longlong), ("grid_evictions", ctypes.c_longlong),
+                ("jobs_submitted", ctypes.c_longlong), ("jobs_admitted", ctypes.c_longlong),
+                ("jobs_done", ctypes.c_longlong), ("jobs_failed", ctypes.c_longlong),
+                ("iterations", ctypes.c_longlong), ("tiles", ctypes.c_longlong),
+                ("kernel_launches", ctypes.c_longlong)]
+
+
+SLOTH_JOB_PENDING, SLOTH_JOB_RUNNING, SLOTH_JOB_DONE, SLOTH_JOB_FETCHING, SLOTH_JOB_FETCHED = 0, 1, 2, 3, 4
+
 # name -> (restype, argtypes); every symbol include/sloth_b200.h declares.
 _SIGNATURES = {
     "sloth_strerror": (c_char_p, [c_int]),
@@ -88,6 +104,16 @@ _SIGNATURES = {
                                 c_int64, POINTER(SlothTraceOutputs), c_void_p, c_size_t, c_void_p]),
     "sloth_trace_f32_noalloc": (c_int, [POINTER(SlothGridDesc), c_void_p, POINTER(SlothTraceParams), c_void_p,
                                         c_int64, POINTER(SlothTraceOutputs), c_void_p]),
+    "sloth_server_create": (c_int, [POINTER(SlothServerConfig), POINTER(c_void_p)]),
+    "sloth_server_destroy": (c_int, [c_void_p]),
+    "sloth_server_submit": (c_int, [c_void_p, ctypes.c_uint64, POINTER(SlothGridDesc), c_void_p, c_int,
+                                    POINTER(SlothTraceParams), c_void_p, c_int, c_int64, POINTER(c_int)]),
+    "sloth_server_step": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
+    "sloth_server_job_state": (c_int, [c_void_p, c_int, POINTER(c_int)]),
+    "sloth_server_fetch": (c_int, [c_void_p, c_int, POINTER(SlothTraceOutputs)]),
+    "sloth_server_release": (c_int, [c_void_p, c_int]),
+    "sloth_server_stats": (c_int, [c_void_p, POINTER(SlothServerStats)]),
+    "sloth_server_sync": (c_int, [c_void_p]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGNATURES)

@@ -1,0 +1,873 @@
+// Device code shared by the tracer entry points (trace.cu) and the request
+// server (server.cu): kernel arguments, samplers, the RK4 step, per-ray
+// bookkeeping, the per-tile tracing loop and the Morton pre-pass.
+//
+// What the reference does (src/core/propagator.py):
+//   dsdt (:168-243): ds/dt = (v, grad(G)(r) [, kappa(r)]), G = -c^2/2 * ne/nc,
+//                    grad(G) from precomputed grids through the trilinear
+//                    interpolator (fill 0 outside the grid);
+//   solve / trace_and_save_depths (:723-793, :1159-1198): vmap of a diffrax
+//                    solve from t = 0 to the save times; output through
+//                    ray_to_Jonesvector (src/shared/propagation.py:4-90).
+// What runs here: the same ODE with fixed-step RK4 in scaled units (grid
+// cells, cells per step), one thread per ray, plus the optical phase integral
+// of omega*(n - 1) (src/legacy/full_solver.py:341-347, n = sqrt(1 - ne/nc))
+// and the inverse-bremsstrahlung optical depth, both as RK4 quadratures of
+// the stage values, and the Jones-vector projection at each save.
+//
+// Grid faces: the RHS jumps to the outside fill there. A step whose
+// straight-line prediction p + w crosses a face is cut to end on it (RK4 with
+// a fraction phi of the step) and the ray then leaves on a straight line; a
+// step whose prediction ends within kFaceMargin cells of a face, or is cut,
+// samples its stage points clamped into the grid, i.e. it integrates the
+// field's limit from inside, so that no stage sits on the discontinuity.
+//
+// Launch structure (all on the caller's stream):
+//   1. keys_kernel   : Morton key of each ray's entry cell + bucket histogram
+//   2. scan_kernel   : exclusive scan of the bucket counts (one CTA)
+//   3. scatter_kernel: rays into bucket order
+//   4. trace_kernel  : persistent CTAs; each takes a tile of 1024 rays in
+//                      bucket order, sorts it by full key in shared memory,
+//                      and its warps trace the tile; lanes whose ray has
+//                      finished are refilled from the tile with one warp
+//                      ballot + one shared-memory atomic per refill.
+#pragma once
+
+#include <cmath>
+#include <type_traits>
+
+#include "common.cuh"
+
+#ifndef SLOTH_TRACE_THREADS
+#define SLOTH_TRACE_THREADS 256
+#endif
+#ifndef SLOTH_TRACE_MIN_BLOCKS
+#define SLOTH_TRACE_MIN_BLOCKS 2
+#endif
+
+namespace sloth {
+
+constexpr int kThreads = SLOTH_TRACE_THREADS;
+constexpr double kFaceMargin = 0.02;     // cells
+constexpr double kSmallX = 0.05;         // bound on (omega_pe/omega)^2 for the series form of n - 1
+
+// Inverse-bremsstrahlung modes of the tracer.
+enum { IB_OFF = 0, IB_SUBCRITICAL = 1, IB_GENERAL = 2 };
+
+// ---------------------------------------------------------------------------
+// Kernel arguments.
+// ---------------------------------------------------------------------------
+struct TraceArgs {
+    GridGeo geo;
+    const void* grid;
+    const void* rays;          // (6, N) of R
+    long long n;
+    const unsigned* perm;      // bucket-ordered ray ids
+    const unsigned* skeys;     // their keys
+    int* tile_counter;
+    int n_tiles;
+    double origin[3], spacing[3];
+    double w_of_v[3];          // w = v * w_of_v   (cells per step per m/s)
+    double v_of_w[3];          // v = w * v_of_w
+    double S[3];               // -(dtau/h)^2 / 2
+    double phase_scale;        // (omega/c) * dtau / 6
+    double tau_scale;          // kappa_q2 * dtau / 6
+    double cl_w, cl_lo;        // Coulomb log below nc, and max(2, cl_w)
+    double ope2;               // (omega_pe/omega)^2 per unit q
+    double plane;
+    int first_save, save_every, n_saves;
+    int axis, t1, t2;
+    int project;
+    void* jones;
+    void* state;
+    double* phase;
+    void* amp;
+    uint8_t* status;
+    int32_t* steps;
+    unsigned long long* total_steps;
+};
+
+__device__ __forceinline__ double sel3(const double (&v)[3], int i) {
+    return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]);
+}
+
+template <class P>
+struct Ray {
+    typename P::Acc p[3];      // position (cells)
+    typename P::Acc w[3];      // velocity (cells per step)
+    typename P::Acc tau;       // sum of kappa stage combinations
+    double ph;                 // sum of (n-1) stage combinations
+    double lag;                // steps between the ray's time and `step` after an exit step
+    int step, save_j, next_save;
+    unsigned id;
+    bool exited;               // left the grid through a face-clipped step
+};
+
+template <class P>
+struct CellCache {
+    unsigned base;
+    typename P::V c[8];
+};
+
+template <class P>
+struct Sample {
+    typename P::R q, g0, g1, g2, k;
+};
+
+// A cached cell as trilinear polynomials in the in-cell coordinates
+// (fx, fy, fz): per channel T = a + bx fx + by fy + bz fz + cxy fx fy +
+// cxz fx fz + cyz fy fz + cxyz fx fy fz, channels q, dq/du, dq/dv, dq/dw and
+// (when NK = 5) the inverse-bremsstrahlung corner rate.
+template <class P, int NK>
+struct CellPoly {
+    unsigned base;
+    typename P::R t[NK][8];
+};
+
+template <class R>
+__device__ __forceinline__ void poly_coeffs(R (&t)[8], R v0, R v1, R v2, R v3, R v4, R v5, R v6, R v7) {
+    // corner index = 4*dx + 2*dy + dz
+    const R bz = v1 - v0, by = v2 - v0, bx = v4 - v0;
+    const R dyz = v3 - v2, dxz = v5 - v4, dxy = v6 - v4;
+    t[0] = v0;
+    t[1] = bx;
+    t[2] = by;
+    t[3] = bz;
+    t[4] = dxy - by;                       // cxy
+    t[5] = dxz - bz;                       // cxz
+    t[6] = dyz - bz;                       // cyz
+    t[7] = ((v7 - v6) - dxz) - (dyz - bz); // cxyz
+}
+
+template <class R>
+__device__ __forceinline__ R poly_eval(const R (&t)[8], R fx, R fy, R fz) {
+    const R cz = (t[3] + fx * t[5]) + fy * (t[6] + fx * t[7]);   // coefficient of fz
+    const R cy = t[2] + fx * t[4];                               // coefficient of fy (without fz)
+    return ((t[0] + fx * t[1]) + fy * cy) + fz * cz;
+}
+
+// n - 1 for n = sqrt(1 - x), x = (omega_pe/omega)^2. SMALLX (FP32 only, used
+// when x <= kSmallX over the whole grid) takes the binomial series
+// -(x/2 + x^2/8 + x^3/16 + 5x^4/128 + 7x^5/256), whose first omitted term is
+// below 2e-8 of x/2 there, instead of a square root and a division.
+template <class P, bool SMALLX>
+__device__ __forceinline__ typename P::R nm1(typename P::R x) {
+    using R = typename P::R;
+    if constexpr (SMALLX && sizeof(R) == 4) {
+        return -x * (R(0.5) + x * (R(0.125) + x * (R(0.0625) + x * (R(0.0390625) + x * R(0.02734375)))));
+    } else {
+        return P::n_minus_1(x);
+    }
+}
+
+// Inverse-bremsstrahlung rate of one grid point per kappa_q2: q^2 * CL(q),
+// CL = max(2, cl_w - ln(max(omega_pe/omega, 1))) (src/core/propagator.py:155-162).
+template <class P>
+__device__ __forceinline__ typename P::R corner_kappa(const TraceArgs& a, typename P::R q) {
+    using R = typename P::R;
+    const R x = q * (R)a.ope2;
+    const R cl = (x > R(1)) ? fmax(R(2), (R)a.cl_w - R(0.5) * P::log_(x)) : (R)a.cl_lo;
+    return q * q * cl;
+}
+
+// Trilinear sample of the packed grid (rules of src/core/interpolator.py:79-104:
+// cell i = floor(p) clamped to [0, n-2], product weights, fill 0 outside)
+// returning q, the three gradient channels and, when IB, the interpolated
+// inverse-bremsstrahlung rate per kappa_q2. The reference interpolates a
+// kappa grid computed at the grid points (src/core/propagator.py:239,
+// :623-631); with uniform Te and Z that grid is q^2 * CL(q) per point, so its
+// interpolant is the weighted sum of the corner values, formed here from the
+// corners already loaded (CL is constant below the critical density).
+//
+// The point is hi + lo: hi is the ray's running position (large) and lo its
+// compensation plus the stage offset (small). The cell index comes from the
+// rounded sum; the weights from (hi - i) + lo, which resolves the position
+// inside the cell to FP32 relative precision rather than FP32 precision of
+// the absolute position. CLAMP moves the point into the grid first.
+template <class P, int IB, bool CLAMP, class Cache>
+__device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R (&hi)[3],
+                                         const typename P::R (&lo)[3], Sample<P>& out, Cache& cc) {
+    using R = typename P::R;
+    using V = typename P::V;
+    const GridGeo& g = a.geo;
+    R h[3], l[3], p[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        h[x] = hi[x];
+        l[x] = lo[x];
+        p[x] = h[x] + l[x];
+        if constexpr (CLAMP) {
+            const R pc = fmin(fmax(p[x], R(0)), lim_of<R>(g, x));
+            if (pc != p[x]) {
+                h[x] = pc;
+                l[x] = R(0);
+                p[x] = pc;
+            }
+        }
+    }
+    const bool in = (p[0] >= R(0)) & (p[0] <= lim_of<R>(g, 0)) & (p[1] >= R(0)) &
+                    (p[1] <= lim_of<R>(g, 1)) & (p[2] >= R(0)) & (p[2] <= lim_of<R>(g, 2));
+    if (!in) {
+        out.q = out.g0 = out.g1 = out.g2 = out.k = R(0);
+        return;
+    }
+    const int ix = min((int)p[0], g.n[0] - 2);
+    const int iy = min((int)p[1], g.n[1] - 2);
+    const int iz = min((int)p[2], g.n[2] - 2);
+    const R fx = (h[0] - (R)ix) + l[0], fy = (h[1] - (R)iy) + l[1], fz = (h[2] - (R)iz) + l[2];
+    const unsigned b = (unsigned)ix * g.sx + (unsigned)iy * g.sy + (unsigned)iz;
+    if constexpr (P::cell_poly) {
+        if (b != cc.base) {
+            cc.base = b;
+            const V v0 = P::load(a.grid, b), v1 = P::load(a.grid, b + 1u);
+            const V v2 = P::load(a.grid, b + g.sy), v3 = P::load(a.grid, b + g.sy + 1u);
+            const V v4 = P::load(a.grid, b + g.sx), v5 = P::load(a.grid, b + g.sx + 1u);
+            const V v6 = P::load(a.grid, b + g.sx + g.sy), v7 = P::load(a.grid, b + g.sx + g.sy + 1u);
+            poly_coeffs<R>(cc.t[0], v0.x, v1.x, v2.x, v3.x, v4.x, v5.x, v6.x, v7.x);
+            poly_coeffs<R>(cc.t[1], v0.y, v1.y, v2.y, v3.y, v4.y, v5.y, v6.y, v7.y);
+            poly_coeffs<R>(cc.t[2], v0.z, v1.z, v2.z, v3.z, v4.z, v5.z, v6.z, v7.z);
+            poly_coeffs<R>(cc.t[3], v0.w, v1.w, v2.w, v3.w, v4.w, v5.w, v6.w, v7.w);
+            if constexpr (IB == IB_SUBCRITICAL) {
+                poly_coeffs<R>(cc.t[4 % (IB ? 5 : 4)], v0.x * v0.x, v1.x * v1.x, v2.x * v2.x, v3.x * v3.x,
+                               v4.x * v4.x, v5.x * v5.x, v6.x * v6.x, v7.x * v7.x);
+            } else if constexpr (IB == IB_GENERAL) {
+                poly_coeffs<R>(cc.t[4 % (IB ? 5 : 4)], corner_kappa<P>(a, v0.x), corner_kappa<P>(a, v1.x),
+                               corner_kappa<P>(a, v2.x), corner_kappa<P>(a, v3.x), corner_kappa<P>(a, v4.x),
+                               corner_kappa<P>(a, v5.x), corner_kappa<P>(a, v6.x), corner_kappa<P>(a, v7.x));
+            }
+        }
+        out.q = poly_eval<R>(cc.t[0], fx, fy, fz);
+        out.g0 = poly_eval<R>(cc.t[1], fx, fy, fz);
+        out.g1 = poly_eval<R>(cc.t[2], fx, fy, fz);
+        out.g2 = poly_eval<R>(cc.t[3], fx, fy, fz);
+        if constexpr (IB == IB_SUBCRITICAL) {
+            out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz) * (R)a.cl_lo;
+        } else if constexpr (IB == IB_GENERAL) {
+            out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz);
+        } else {
+            out.k = R(0);
+        }
+    } else {
+        V c[8];
+        if constexpr (P::cell_cache) {
+            if (b != cc.base) {
+                cc.base = b;
+                cc.c[0] = P::load(a.grid, b);
+                cc.c[1] = P::load(a.grid, b + 1u);
+                cc.c[2] = P::load(a.grid, b + g.sy);
+                cc.c[3] = P::load(a.grid, b + g.sy + 1u);
+                cc.c[4] = P::load(a.grid, b + g.sx);
+                cc.c[5] = P::load(a.grid, b + g.sx + 1u);
+                cc.c[6] = P::load(a.grid, b + g.sx + g.sy);
+                cc.c[7] = P::load(a.grid, b + g.sx + g.sy + 1u);
+            }
+    #pragma unroll
+            for (int i = 0; i < 8; ++i) c[i] = cc.c[i];
+        } else {
+            c[0] = P::load(a.grid, b);
+            c[1] = P::load(a.grid, b + 1u);
+            c[2] = P::load(a.grid, b + g.sy);
+            c[3] = P::load(a.grid, b + g.sy + 1u);
+            c[4] = P::load(a.grid, b + g.sx);
+            c[5] = P::load(a.grid, b + g.sx + 1u);
+            c[6] = P::load(a.grid, b + g.sx + g.sy);
+            c[7] = P::load(a.grid, b + g.sx + g.sy + 1u);
+        }
+        const R ex = R(1) - fx, ey = R(1) - fy, ez = R(1) - fz;
+        const R w00 = ex * ey, w01 = ex * fy, w10 = fx * ey, w11 = fx * fy;
+        const R w[8] = {w00 * ez, w00 * fz, w01 * ez, w01 * fz, w10 * ez, w10 * fz, w11 * ez, w11 * fz};
+        R q = R(0), g0 = R(0), g1 = R(0), g2 = R(0);
+    #pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            q += c[i].x * w[i];
+            g0 += c[i].y * w[i];
+            g1 += c[i].z * w[i];
+            g2 += c[i].w * w[i];
+        }
+        out.q = q;
+        out.g0 = g0;
+        out.g1 = g1;
+        out.g2 = g2;
+        if constexpr (IB == IB_SUBCRITICAL) {
+            R k = R(0);
+    #pragma unroll
+            for (int i = 0; i < 8; ++i) k += w[i] * (c[i].x * c[i].x);
+            out.k = k * (R)a.cl_lo;
+        } else if constexpr (IB == IB_GENERAL) {
+            R k = R(0);
+    #pragma unroll
+            for (int i = 0; i < 8; ++i) k += w[i] * corner_kappa<P>(a, c[i].x);
+            out.k = k;
+        } else {
+            out.k = R(0);
+        }
+    }
+}
+
+// One RK4 step of length phi (in steps; phi = 1 except for a step cut at a
+// grid face) in scaled units; see the file header. Stage sums are
+// accumulated as the stages are produced to keep few values live:
+//   p' = p + phi*w + phi^2 (A1 + A2 + A3)/6,  w' = w + phi (A1 + 2A2 + 2A3 + A4)/6,
+//   stage points p, p + phi*w/2, p + phi*w2/2, p + phi*w3
+//   with w2 = w + phi*A1/2, w3 = w + phi*A2/2.
+// The phase integrand is n - 1 with n = sqrt(1 - (omega_pe/omega)^2) from the
+// interpolated density (src/legacy/full_solver.py:271-274, :341-347).
+template <class P, int IB, bool SMALLX, bool CLAMP, class Cache>
+__device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
+    using R = typename P::R;
+    const R two = R(2);
+    const R hphi = R(0.5) * phi, phi6 = phi * R(1.0 / 6.0), phi2_6 = phi * phi6;
+    const R S0 = (R)a.S[0], S1 = (R)a.S[1], S2 = (R)a.S[2];
+    const R ope2 = (R)a.ope2;
+    R ph[3], pl[3], we[3], sA[3], sW[3], w3[3], st[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        ph[x] = r.p[x].hi();
+        pl[x] = r.p[x].lo();
+        we[x] = r.w[x].val();
+    }
+    Sample<P> s;
+    // stage 1 at p
+    sample_c<P, IB, CLAMP>(a, ph, pl, s, cc);
+    R g = nm1<P, SMALLX>(ope2 * s.q);
+    R kq = s.k;
+    sA[0] = S0 * s.g0; sA[1] = S1 * s.g1; sA[2] = S2 * s.g2;
+    // stage 2 at p + phi*w/2
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        sW[x] = sA[x];
+        st[x] = pl[x] + hphi * we[x];
+    }
+    sample_c<P, IB, CLAMP>(a, ph, st, s, cc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + hphi * (we[x] + hphi * sA[x]);   // p + phi*w2/2
+    {
+        const R A[3] = {S0 * s.g0, S1 * s.g1, S2 * s.g2};
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            w3[x] = we[x] + hphi * A[x];
+            sA[x] += A[x];
+            sW[x] += two * A[x];
+        }
+    }
+    g += two * nm1<P, SMALLX>(ope2 * s.q);
+    kq += two * s.k;
+    // stage 3 at p + phi*w2/2
+    sample_c<P, IB, CLAMP>(a, ph, st, s, cc);
+    {
+        const R A[3] = {S0 * s.g0, S1 * s.g1, S2 * s.g2};
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            sA[x] += A[x];
+            sW[x] += two * A[x];
+            st[x] = pl[x] + phi * w3[x];
+        }
+    }
+    g += two * nm1<P, SMALLX>(ope2 * s.q);
+    kq += two * s.k;
+    // stage 4 at p + phi*w3
+    sample_c<P, IB, CLAMP>(a, ph, st, s, cc);
+    sW[0] += S0 * s.g0; sW[1] += S1 * s.g1; sW[2] += S2 * s.g2;
+    g += nm1<P, SMALLX>(ope2 * s.q);
+    kq += s.k;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        const R dp = phi * r.w[x].hi() + (phi * r.w[x].lo() + phi2_6 * sA[x]);
+        r.p[x].add(dp);
+        r.w[x].add(phi6 * sW[x]);
+    }
+    r.ph += (double)(phi * g);
+    if constexpr (IB != IB_OFF) r.tau.add(phi * kq);
+}
+
+// Kind of the next step of a ray: 0 plain step of a ray inside the grid whose
+// prediction stays more than kFaceMargin inside; 1 full step sampled with
+// clamped stage points (its prediction ends within kFaceMargin of a face);
+// 2 step cut at the face its prediction crosses, length phi, after which the
+// ray leaves; 3 plain step of a ray outside the grid (zero RHS).
+template <class P>
+__device__ __forceinline__ int step_kind(const TraceArgs& a, const Ray<P>& r, typename P::R& phi) {
+    using R = typename P::R;
+    const R margin = R(kFaceMargin);
+    R p[3], w[3];
+    bool in = true;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        p[x] = r.p[x].val();
+        w[x] = r.w[x].val();
+        in = in & (p[x] >= R(0)) & (p[x] <= lim_of<R>(a.geo, x));
+    }
+    phi = R(1);
+    if (!in) return 3;
+    bool near = false;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        const R pn = p[x] + w[x];
+        const R lim = lim_of<R>(a.geo, x);
+        if (pn > lim - margin) {
+            near = true;
+            // distance to the face from the compensated position
+            if (pn > lim) phi = fmin(phi, ((lim - r.p[x].hi()) - r.p[x].lo()) / w[x]);
+        }
+        if (pn < margin) {
+            near = true;
+            if (pn < R(0)) phi = fmin(phi, (-r.p[x].hi() - r.p[x].lo()) / w[x]);
+        }
+    }
+    phi = fmax(phi, R(0));
+    return phi < R(1) ? 2 : (near ? 1 : 0);
+}
+
+template <class P>
+__device__ __forceinline__ bool ray_in_grid(const TraceArgs& a, const Ray<P>& r) {
+    using R = typename P::R;
+    bool in = true;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        const R p = r.p[x].val();
+        in = in & (p >= R(0)) & (p <= lim_of<R>(a.geo, x));
+    }
+    return in;
+}
+
+// True once the ray is outside the grid on an axis and moving away from it
+// on that axis: its path is then a straight line that never re-enters.
+template <class P>
+__device__ __forceinline__ bool ray_gone(const TraceArgs& a, const Ray<P>& r) {
+    using R = typename P::R;
+    bool gone = false;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        const R p = r.p[x].val(), w = r.w[x].val();
+        gone = gone | ((p < R(0)) & (w <= R(0))) | ((p > lim_of<R>(a.geo, x)) & (w >= R(0)));
+    }
+    return gone;
+}
+
+// Writes save j of ray `id` from its state (cells, cells per step, FP64)
+// `drift` unit steps before the save time (drift > 0 only for rays that have
+// left the grid for good, whose path is a straight line).
+template <class R>
+__device__ __forceinline__ void emit_save(const TraceArgs& a, unsigned id, int j, double drift,
+                                       double p0, double p1, double p2, double w0, double w1,
+                                       double w2, double ph, double tau) {
+    double x[3], v[3];
+    const double p[3] = {p0, p1, p2}, w[3] = {w0, w1, w2};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        x[k] = a.origin[k] + (p[k] + drift * w[k]) * a.spacing[k];
+        v[k] = w[k] * a.v_of_w[k];
+    }
+    const double xa = sel3(x, a.axis), va = sel3(v, a.axis);
+    const double x1 = sel3(x, a.t1), v1 = sel3(v, a.t1);
+    const double x2 = sel3(x, a.t2), v2 = sel3(v, a.t2);
+    double pos1 = x1, pos2 = x2;
+    if (a.project) {
+        const double tbp = (xa - a.plane) / va;
+        pos1 = x1 - v1 * tbp;
+        pos2 = x2 - v2 * tbp;
+    }
+    const size_t n = (size_t)a.n;
+    R* jo = reinterpret_cast<R*>(a.jones) + (size_t)j * 4u * n;
+    jo[id] = (R)pos1;
+    jo[n + id] = (R)atan(v1 / va);
+    jo[2 * n + id] = (R)pos2;
+    jo[3 * n + id] = (R)atan(v2 / va);
+    if (a.state) {
+        R* so = reinterpret_cast<R*>(a.state) + (size_t)j * 6u * n;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            so[k * n + id] = (R)x[k];
+            so[(3 + k) * n + id] = (R)v[k];
+        }
+    }
+    if (a.phase) a.phase[(size_t)j * n + id] = ph * a.phase_scale;
+    if (a.amp) reinterpret_cast<R*>(a.amp)[(size_t)j * n + id] = (R)exp(-tau * a.tau_scale);
+}
+
+template <class P>
+__device__ __forceinline__ void emit(const TraceArgs& a, const Ray<P>& r, double drift) {
+    emit_save<typename P::R>(a, r.id, r.save_j, drift, r.p[0].vald(), r.p[1].vald(), r.p[2].vald(),
+                             r.w[0].vald(), r.w[1].vald(), r.w[2].vald(), r.ph, r.tau.vald());
+}
+
+template <class P>
+__device__ __forceinline__ void finish_ray(const TraceArgs& a, const Ray<P>& r, uint8_t st,
+                                           unsigned long long& my_steps) {
+    bool finite = isfinite(r.ph);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) finite = finite & isfinite(r.p[k].vald()) & isfinite(r.w[k].vald());
+    if (!finite) st = SLOTH_RAY_NONFINITE;
+    if (a.status) a.status[r.id] = st;
+    if (a.steps) a.steps[r.id] = r.step;
+    my_steps += (unsigned long long)r.step;
+}
+
+// Saves due at the current step, then the end / exit checks. Returns true
+// while the ray still needs steps. `check_gone` is false after a plain step
+// taken from inside the grid with its prediction more than kFaceMargin inside
+// (the ray cannot have left); the outside test is skipped then.
+template <class P>
+__device__ __forceinline__ bool settle(const TraceArgs& a, Ray<P>& r, unsigned long long& my_steps,
+                                      bool check_gone = true) {
+    while (r.save_j < a.n_saves && r.next_save == r.step) {
+        emit<P>(a, r, r.lag);
+        ++r.save_j;
+        r.next_save += a.save_every;
+    }
+    if (r.save_j >= a.n_saves) {
+        finish_ray<P>(a, r, (!r.exited && ray_in_grid<P>(a, r)) ? SLOTH_RAY_INSIDE_AT_END : SLOTH_RAY_EXITED,
+                      my_steps);
+        return false;
+    }
+    if (r.exited || (check_gone && ray_gone<P>(a, r))) {
+        while (r.save_j < a.n_saves) {
+            emit<P>(a, r, (double)(r.next_save - r.step) + r.lag);
+            ++r.save_j;
+            r.next_save += a.save_every;
+        }
+        finish_ray<P>(a, r, SLOTH_RAY_EXITED, my_steps);
+        return false;
+    }
+    return true;
+}
+
+template <class P>
+__device__ __forceinline__ bool start_ray(const TraceArgs& a, unsigned id, Ray<P>& r,
+                                          unsigned long long& my_steps) {
+    using R = typename P::R;
+    const R* rays = reinterpret_cast<const R*>(a.rays);
+    const size_t n = (size_t)a.n;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double x = (double)rays[k * n + id];
+        const double v = (double)rays[(3 + k) * n + id];
+        r.p[k].set((x - a.origin[k]) / a.spacing[k]);
+        r.w[k].set(v * a.w_of_v[k]);
+    }
+    r.tau.set(0.0);
+    r.ph = 0.0;
+    r.lag = 0.0;
+    r.exited = false;
+    r.step = 0;
+    r.save_j = 0;
+    r.next_save = a.first_save;
+    r.id = id;
+    return settle<P>(a, r, my_steps);
+}
+
+// Shared-memory bitonic sort of (key, id) pairs, ascending by key then id.
+__device__ __forceinline__ void tile_sort(unsigned* key, unsigned* id) {
+    for (int k = 2; k <= kTile; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const unsigned ki = key[i], kl = key[l], ii = id[i], il = id[l];
+                    const bool gt = (ki > kl) || (ki == kl && ii > il);
+                    const bool up = (i & k) == 0;
+                    if (gt == up) {
+                        key[i] = kl; key[l] = ki;
+                        id[i] = il; id[l] = ii;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Traces one tile of `cnt` rays (bucket-ordered ids perm[start..], keys
+// skeys[start..]): sorts them by key in shared memory, then the block's warps
+// trace them one thread per ray, refilling finished lanes from the tile
+// (warp ballot + shared-memory atomic). *s_head must be 0 on entry and the
+// block must be synchronised. Shared by the single-trace and serving kernels.
+template <class P, int IB, bool SMALLX, class Cache>
+__device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, int cnt, unsigned* s_key,
+                                           unsigned* s_id, int* s_head, Cache& cc,
+                                           unsigned long long& my_steps) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
+        if (i < cnt) {
+            s_key[i] = a.skeys[start + i];
+            s_id[i] = a.perm[start + i];
+        } else {
+            s_key[i] = 0xffffffffu;
+            s_id[i] = 0xffffffffu;
+        }
+    }
+    __syncthreads();
+    tile_sort(s_key, s_id);
+
+    Ray<P> r;
+    bool active = false, qempty = false;
+    for (;;) {
+        const unsigned idle = __ballot_sync(FULL, !active);
+        if (idle != 0u && !qempty) {
+            const int nidle = __popc(idle);
+            const int leader = __ffs(idle) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(s_head, nidle);
+            base = __shfl_sync(FULL, base, leader);
+            if (base + nidle >= cnt) qempty = true;
+            if (!active) {
+                const int kk = base + __popc(idle & lt_mask);
+                if (kk < cnt) active = start_ray<P>(a, s_id[kk], r, my_steps);
+            }
+        }
+        if (__ballot_sync(FULL, active) == 0u) {
+            if (qempty) break;
+            continue;
+        }
+        if (active) {
+            typename P::R phi;
+            const int kind = step_kind<P>(a, r, phi);
+            if (kind == 0 || kind == 3) {
+                rk4_step<P, IB, SMALLX, false>(a, r, cc, typename P::R(1));
+            } else {
+                rk4_step<P, IB, SMALLX, true>(a, r, cc, phi);
+                if (kind == 2) {
+                    r.exited = true;
+                    r.lag = 1.0 - (double)phi;
+                }
+            }
+            ++r.step;
+            active = settle<P>(a, r, my_steps, kind != 0);
+        }
+    }
+    __syncthreads();
+}
+
+// Register cache of the last cell: polynomial coefficients or corners.
+template <class P, int IB>
+using CellCacheFor = typename std::conditional<P::cell_poly, CellPoly<P, (IB != IB_OFF) ? 5 : 4>, CellCache<P>>::type;
+
+// Sum of `v` over the block, added to *dst by one thread.
+__device__ __forceinline__ void block_add(unsigned long long v, unsigned long long* s_acc,
+                                          unsigned long long* dst) {
+    const unsigned FULL = 0xffffffffu;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(s_acc, v);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (dst && *s_acc) atomicAdd(dst, *s_acc);
+        *s_acc = 0;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Morton bucket pre-pass.
+// ---------------------------------------------------------------------------
+struct KeyArgs {
+    const void* rays;
+    long long n;
+    double origin[3], inv_h[3];
+    int cmax[3];      // n - 2 per axis
+    int shift[3];     // right shift to fit 10 bits
+    int axis, t1, t2;
+    int bucket_shift; // key >> bucket_shift = bucket
+    unsigned* keys;
+    unsigned* hist;
+};
+
+template <class R>
+__global__ void __launch_bounds__(256) keys_kernel(const KeyArgs k) {
+    const R* rays = reinterpret_cast<const R*>(k.rays);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < k.n; i += stride) {
+        unsigned c[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            double u = floor(((double)rays[a * k.n + i] - k.origin[a]) * k.inv_h[a]);
+            u = fmin(fmax(u, 0.0), (double)k.cmax[a]);   // NaN -> 0
+            c[a] = ((unsigned)u) >> k.shift[a];
+        }
+        const unsigned c1 = k.t1 == 0 ? c[0] : c[1];
+        const unsigned c2 = k.t2 == 1 ? c[1] : c[2];
+        const unsigned ca = k.axis == 0 ? c[0] : (k.axis == 1 ? c[1] : c[2]);
+        const unsigned key = morton_key(c1, c2, ca);
+        k.keys[i] = key;
+        atomicAdd(k.hist + (key >> k.bucket_shift), 1u);
+    }
+}
+
+// Exclusive scan of nb (<= 2^18) counts by one CTA of 1024 threads.
+static __global__ void __launch_bounds__(1024) scan_kernel(unsigned* hist, int nb) {
+    __shared__ unsigned s_warp[32];
+    const int t = threadIdx.x;
+    const int per = (nb + 1023) / 1024;
+    const int lo = min(t * per, nb), hi = min(lo + per, nb);
+    unsigned sum = 0;
+    for (int i = lo; i < hi; ++i) sum += hist[i];
+    // block exclusive scan of the per-thread sums
+    unsigned inc = sum;
+    const int lane = t & 31, wid = t >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_warp[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned v = s_warp[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        s_warp[lane] = v;
+    }
+    __syncthreads();
+    unsigned run = inc - sum + (wid > 0 ? s_warp[wid - 1] : 0u);
+    for (int i = lo; i < hi; ++i) {
+        const unsigned c = hist[i];
+        hist[i] = run;
+        run += c;
+    }
+}
+
+static __global__ void __launch_bounds__(256) scatter_kernel(const unsigned* __restrict__ keys, long long n,
+                                                      int bucket_shift, unsigned* offs,
+                                                      unsigned* __restrict__ perm,
+                                                      unsigned* __restrict__ skeys) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const unsigned key = keys[i];
+        const unsigned pos = atomicAdd(offs + (key >> bucket_shift), 1u);
+        perm[pos] = (unsigned)i;
+        skeys[pos] = key;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+inline size_t align256(size_t x) { return (x + 255u) & ~(size_t)255u; }
+
+constexpr size_t kHeaderBytes = 256;
+constexpr size_t kHistBytes = (size_t)4 << kMaxBucketBits;
+
+inline size_t workspace_bytes(long long n) {
+    const size_t a = align256((size_t)(n > 0 ? n : 1) * 4u);
+    return kHeaderBytes + kHistBytes + 3 * a;
+}
+
+inline int bucket_bits_for(long long n) {
+    int bits = 0;
+    while (bits < kMaxBucketBits && ((long long)1 << bits) * 32 < n) ++bits;
+    return bits;
+}
+
+
+// Morton pre-pass of n rays into bucket order: keys, histogram (2^bbits
+// buckets, zeroed by the caller), exclusive scan, scatter into perm/skeys.
+template <class R>
+inline int launch_prepass(const SlothGridDesc* g, int axis, const R* rays, long long n, int bbits,
+                          unsigned* keys, unsigned* hist, unsigned* perm, unsigned* skeys, int sms,
+                          cudaStream_t s) {
+    const int t1 = axis == 0 ? 1 : 0;
+    const int t2 = axis == 2 ? 1 : 2;
+    KeyArgs ka;
+    ka.rays = rays;
+    ka.n = n;
+    for (int k = 0; k < 3; ++k) {
+        ka.origin[k] = g->origin[k];
+        ka.inv_h[k] = 1.0 / g->spacing[k];
+        ka.cmax[k] = g->n[k] - 2;
+        int sh = 0;
+        while (((g->n[k] - 2) >> sh) > 1023) ++sh;
+        ka.shift[k] = sh;
+    }
+    ka.axis = axis;
+    ka.t1 = t1;
+    ka.t2 = t2;
+    ka.bucket_shift = 30 - bbits;
+    ka.keys = keys;
+    ka.hist = hist;
+    const long long nblk = (n + 255) / 256;
+    const int kb = (int)(nblk < (long long)sms * 8 ? nblk : (long long)sms * 8);
+    keys_kernel<R><<<kb, 256, 0, s>>>(ka);
+    note_launch();
+    scan_kernel<<<1, 1024, 0, s>>>(hist, 1 << bbits);
+    note_launch();
+    scatter_kernel<<<kb, 256, 0, s>>>(keys, n, 30 - bbits, hist, perm, skeys);
+    note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+// Kernel arguments of one trace from the public descriptors.
+inline void fill_trace_args(TraceArgs& ta, const SlothGridDesc* g, const void* grid, const SlothTraceParams* p,
+                            const void* rays, long long n, const SlothTraceOutputs* out, const unsigned* perm,
+                            const unsigned* skeys) {
+    const int axis = p->probing_axis;
+    ta.geo = make_geo(g);
+    ta.grid = grid;
+    ta.rays = rays;
+    ta.n = n;
+    ta.perm = perm;
+    ta.skeys = skeys;
+    ta.tile_counter = nullptr;
+    ta.n_tiles = (int)((n + kTile - 1) / kTile);
+    for (int k = 0; k < 3; ++k) {
+        const double h = g->spacing[k];
+        ta.origin[k] = g->origin[k];
+        ta.spacing[k] = h;
+        ta.w_of_v[k] = (p->dtau / h) / kC;
+        ta.v_of_w[k] = kC * h / p->dtau;
+        ta.S[k] = -0.5 * (p->dtau / h) * (p->dtau / h);
+    }
+    ta.phase_scale = (p->omega / kC) * p->dtau / 6.0;
+    ta.tau_scale = p->kappa_q2 * p->dtau / 6.0;
+    ta.cl_w = p->coulomb_log_w;
+    ta.cl_lo = p->coulomb_log_w > 2.0 ? p->coulomb_log_w : 2.0;
+    ta.ope2 = p->ope_ratio2;
+    ta.plane = p->plane;
+    ta.first_save = p->first_save;
+    ta.save_every = p->n_saves > 1 ? p->save_every : 1;
+    ta.n_saves = p->n_saves;
+    ta.axis = axis;
+    ta.t1 = axis == 0 ? 1 : 0;
+    ta.t2 = axis == 2 ? 1 : 2;
+    ta.project = p->project_to_plane ? 1 : 0;
+    ta.jones = out->jones;
+    ta.state = out->state;
+    ta.phase = out->phase;
+    ta.amp = out->amp;
+    ta.status = out->status;
+    ta.steps = out->steps;
+    ta.total_steps = out->total_steps;
+}
+
+// Validation shared by the trace entry points (everything but buffers).
+inline int check_trace_params(const SlothGridDesc* g, const SlothTraceParams* p, int64_t n) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (!p) return SLOTH_ERR_NULL_POINTER;
+    if (n < 0 || n > 2147483647LL) return n < 0 ? SLOTH_ERR_INVALID_ARGUMENT : SLOTH_ERR_TOO_LARGE;
+    if (!(p->omega > 0.0) || !(p->dtau > 0.0) || !std::isfinite(p->dtau) || !std::isfinite(p->omega))
+        return SLOTH_ERR_INVALID_ARGUMENT;
+    if (p->n_saves < 1 || p->n_saves > SLOTH_MAX_SAVES || p->first_save < 0) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (p->n_saves > 1 && p->save_every < 1) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (p->probing_axis < 0 || p->probing_axis > 2) return SLOTH_ERR_INVALID_ARGUMENT;
+    const long long last =
+        (long long)p->first_save + (long long)(p->n_saves - 1) * (p->n_saves > 1 ? p->save_every : 0);
+    if (last > 2000000000LL) return SLOTH_ERR_TOO_LARGE;
+    if (p->inv_brems && !(p->kappa_q2 >= 0.0)) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (p->project_to_plane && !std::isfinite(p->plane)) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (!std::isfinite(p->q_max)) return SLOTH_ERR_INVALID_ARGUMENT;
+    return SLOTH_OK;
+}
+
+// Tracer mode of a trace: inverse-bremsstrahlung path and phase form.
+inline void trace_mode(const SlothTraceParams* p, int* ib, bool* smallx) {
+    const double xmax = p->q_max > 0.0 ? p->q_max * p->ope_ratio2 : 1e300;
+    *smallx = xmax <= kSmallX;
+    *ib = !p->inv_brems ? IB_OFF : (xmax <= 1.0 ? IB_SUBCRITICAL : IB_GENERAL);
+}
+
+}  // namespace sloth

@@ -1,0 +1,112 @@
+"""Request server: continuous batching of mixed jobs, HBM-budget admission,
+grid residency, and results that are the same alone and in the mix."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from sloth_b200 import _capi, runtime, serving, workloads
+from sloth_b200.core import physics
+
+pytestmark = pytest.mark.gpu
+
+L = 5e-3
+LWL = 532e-9
+
+
+def _job_specs():
+    # (kind, n, rays, seed): mixed grid sizes, ray counts and tracer modes
+    return [("kolmogorov", 48, 5000, 1), ("sinusoid", 64, 3000, 2), ("kolmogorov", 32, 20000, 3),
+            ("sinusoid", 40, 1500, 4), ("kolmogorov", 48, 700, 5), ("sinusoid", 64, 12000, 6)]
+
+
+def _fields(specs):
+    return {serving.grid_key(k, n, 0): serving.field_for(k, n, 0, L=L) for k, n, _, _ in specs}
+
+
+def _submit(srv, fields, kind, n, nrays, seed):
+    rays = workloads.gaussian_beam(nrays, waist=2e-3, L=L, seed=seed, jitter=1e-3, device="cuda")
+    key = serving.grid_key(kind, n, 0)
+    h = L / (n - 1)
+    kol = kind == "kolmogorov"
+    return srv.submit(key, fields[key], (-L / 2,) * 3, (h,) * 3, (n,) * 3, rays, lwl=LWL, detector_plane=L / 2,
+                      inv_brems=kol, Te=20.0, Z=1.0), rays
+
+
+def _direct(fields, kind, n, rays):
+    """The same trace through the single-trace entry point."""
+    key = serving.grid_key(kind, n, 0)
+    h = L / (n - 1)
+    g = runtime.pack_grid(fields[key], (-L / 2,) * 3, (h,) * 3, physics.omega_of(LWL))
+    sched = runtime.schedule_times([math.sqrt(8.0) * (L)], (h, h, h))
+    kol = kind == "kolmogorov"
+    out = runtime.trace(g, rays, sched, project=True, plane=L / 2, inv_brems=kol, Te=20.0, Z=1.0)
+    torch.cuda.synchronize()
+    return {k: v.cpu() for k, v in out.items()}
+
+
+def _same(a, b):
+    assert torch.equal(a["jones"], b["jones"])
+    assert torch.equal(a["phase"], b["phase"])
+    assert torch.equal(a["steps"], b["steps"]) and torch.equal(a["status"], b["status"])
+    if "amp" in b:
+        assert torch.equal(a["amp"], b["amp"])
+    assert int(a["total_steps"][0]) == int(b["total_steps"][0])
+
+
+def test_results_same_alone_and_in_the_mix():
+    specs = _job_specs()
+    fields = _fields(specs)
+    with serving.RayServer(2 << 30, tiles_per_step=64, quantum=2) as srv:
+        alone = []
+        for kind, n, nr, seed in specs:
+            job, rays = _submit(srv, fields, kind, n, nr, seed)
+            srv.run_until_done([job])
+            alone.append((job.out, rays))
+            srv.release(job)
+        mixed = [_submit(srv, fields, kind, n, nr, seed)[0] for kind, n, nr, seed in specs]
+        srv.run_until_done(mixed)
+        st = srv.stats()
+        assert st["grid_packs"] == len({(k, n) for k, n, _, _ in specs})   # grids stayed resident
+    for (kind, n, _, _), (a, rays), m in zip(specs, alone, mixed):
+        _same(m.out, a)
+        _same(a, _direct(fields, kind, n, rays))
+
+
+def test_budget_admission_and_eviction():
+    # an 80^3 grid (8.2 MB) and a 96^3 grid (14.2 MB) with their jobs (~2.8 MB
+    # each) do not fit in 24 MB together: the 96^3 jobs wait until the 80^3
+    # jobs are done, and the idle 80^3 grid is evicted to make room
+    specs = [("kolmogorov", 80, 40000, s) for s in range(3)] + [("sinusoid", 96, 40000, s) for s in range(3)]
+    fields = {}
+    for k, n, _, _ in specs:
+        fields[serving.grid_key(k, n, 0)] = serving.field_for(k, n, 0, L=L)
+    budget = 24 << 20
+    with serving.RayServer(budget, tiles_per_step=32) as srv:
+        jobs = [_submit(srv, fields, k, n, nr, seed) for k, n, nr, seed in specs]
+        res = srv.run_until_done([j for j, _ in jobs])
+        st = srv.stats()
+        assert st["arena_used"] <= st["budget_bytes"]
+        assert st["jobs_done"] == len(specs) and st["jobs_failed"] == 0
+        assert st["grid_evictions"] >= 1
+    for (kind, n, _, _), (job, rays) in zip(specs, jobs):
+        _same(res[job.id], _direct(fields, kind, n, rays))
+
+
+def test_job_that_can_never_fit_is_refused():
+    fields = {serving.grid_key("sinusoid", 128, 0): serving.field_for("sinusoid", 128, 0, L=L)}
+    with serving.RayServer(16 << 20) as srv:
+        with pytest.raises(_capi.SlothError) as e:
+            _submit(srv, fields, "sinusoid", 128, 1000, 0)     # 128^3 grid = 33.5 MB > 16 MB
+        assert e.value.code == _capi.SLOTH_ERR_TOO_LARGE
+
+
+def test_short_request_stream():
+    reqs = serving.request_stream(40, rate=400.0, sizes=(32, 48, 64), ray_median=5e3, ray_min=500, ray_max=4e4,
+                                  seed=3)
+    with serving.RayServer(4 << 30) as srv:
+        res = serving.replay(srv, reqs)
+    assert res["requests"] == 40
+    assert res["p99_ms"] >= res["p50_ms"] > 0
+    assert res["ray_steps"] > 0 and res["stats"]["iterations"] >= 1

@@ -154,3 +154,21 @@ def test_beams_and_profiles():
     assert s.shape == (16, 16, 16) and float(s.max()) <= 1.1e24 * (1 + 1e-6)
     t = workloads.parabolic_trough(16)
     assert float(t.min()) >= 5e24 * (1 - 1e-6)
+
+
+def test_serving_request_stream_statistics():
+    from sloth_b200 import serving
+    reqs = serving.request_stream(2000, rate=200.0, seed=0)
+    t = np.array([r.t for r in reqs])
+    assert np.all(np.diff(t) >= 0) and t[0] == 0.0
+    assert abs(len(reqs) / t[-1] - 200.0) < 15.0                       # Poisson rate
+    rays = np.array([r.rays for r in reqs])
+    assert rays.min() >= 1e4 and rays.max() <= 4e6
+    assert 1.6e5 < np.median(rays) < 2.5e5                             # lognormal median 2e5
+    sizes = np.array([r.n for r in reqs])
+    assert set(sizes) == {64, 128, 192, 256, 384}
+    kinds = np.array([r.kind for r in reqs])
+    assert 0.45 < (kinds == "kolmogorov").mean() < 0.55
+    assert serving.request_stream(5, seed=1)[3] == serving.request_stream(5, seed=1)[3]
+    keys = {serving.grid_key(r.kind, r.n, r.field_seed) for r in reqs}
+    assert len(keys) <= 20
