@@ -64,10 +64,11 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def committed_traffic():
-    """DRAM bytes per trace launch from the committed ncu summary, if any."""
+def committed_traffic(args):
+    """DRAM bytes per trace launch from the committed ncu summary of the
+    512^3 / 1e7-ray workload (None for any other workload)."""
     p = os.path.join(ROOT, "profiles", "trace_kernel_kolmogorov512_1e7.md")
-    if not os.path.exists(p):
+    if (args.n, int(args.rays), args.seed) != (512, 10 ** 7, 2024) or not os.path.exists(p):
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
     return float(m.group(1)) if m else None
@@ -416,7 +417,7 @@ def run_sloth(args):
         peak, peak_kind = measured_peaks()
         kms = float(np.mean(kernel_ms))
         achieved = ray_steps * BYTES_PER_RAY_STEP / (kms / 1e3) / 1e9
-        traffic = committed_traffic()
+        traffic = committed_traffic(args)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -424,7 +425,8 @@ def run_sloth(args):
             "config": {"workload": f"{n}^3 Kolmogorov turbulent box (mean 1e19 cm^-3, 20% RMS, k^-11/3), "
                                    f"{nrays:.0e} rays, 3 mm Gaussian beam along +z, 532 nm, Te=20 eV, Z=1, "
                                    "fixed-step RK4 ds=h/2, detector plane z=+2.5 mm",
-                       "l2": "inputs larger than L2 (2.1 GB packed grid, 240 MB rays)",
+                       "l2": f"inputs larger than L2 ({n ** 3 * 16 / 1e9:.2f} GB packed grid, "
+                             f"{nrays * 24 / 1e6:.0f} MB rays)",
                        "precision": "FP32 state with compensated sums, FP64 phase, Kahan FP32 optical depth",
                        "seed": args.seed, "ray_steps_per_trace": ray_steps},
             "latency_ms": {"p50": float(np.percentile(per_step_ms, 50)), "p99": float(np.percentile(per_step_ms, 99)),
