@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=2000)
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -242,6 +243,74 @@ def run_serving(args):
 
 
 # ---------------------------------------------------------------------------
+# adjoint: d loss / d ne for a 256^2 detector image of 1e6 rays through a
+# 128^3 FP32 Kolmogorov grid (400 RK4 steps, checkpoints every 20, 2-pixel
+# splat); loss = ||I - I_target||^2 with I_target from another seeded field
+# ---------------------------------------------------------------------------
+def run_adjoint(args):
+    import torch
+    from sloth_b200 import adjoint, workloads
+    n, nrays = 128, 1_000_000
+    h = L / (n - 1)
+    spec = adjoint.box_detector(L, n_px=256, sigma_px=2.0, n_steps=400, ckpt_every=20)
+    ne_t = workloads.kolmogorov_box(n, L=L, mean=1e25, rms=0.2, seed=args.seed + 41, device="cuda")
+    ne = workloads.kolmogorov_box(n, L=L, mean=1e25, rms=0.2, seed=args.seed + 42, device="cuda")
+    rays = workloads.gaussian_beam(nrays, waist=1.5e-3, L=L, seed=args.seed + 43, device="cuda")
+    kw = dict(origin=(-L / 2,) * 3, spacing=(h,) * 3, lwl=LWL)
+    with torch.no_grad():
+        target = adjoint.detector_image(ne_t, rays, spec, **kw, precision="f64").double()
+    stream = torch.cuda.current_stream()
+    fwd_ms, bwd_ms, steps = [], [], 0
+    for it in range(3 + max(args.steps, 3)):
+        x = ne.detach().requires_grad_(True)
+        st = {}
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        img = adjoint.detector_image(x, rays, spec, **kw, precision="f32", stats=st)
+        e1.record(stream)
+        loss = (img.double() - target).pow(2).sum()
+        loss.backward()
+        e2.record(stream)
+        torch.cuda.synchronize()
+        if it >= 3:
+            fwd_ms.append(e0.elapsed_time(e1))
+            bwd_ms.append(e1.elapsed_time(e2))
+            steps = int(st["ray_steps"][0])
+    g32 = x.grad.double()
+    # central differences of the FP64 forward at 16 voxels of the beam's core
+    rng = np.random.default_rng(args.seed)
+    c = n // 2
+    vox = [tuple(int(v) for v in rng.integers(c - 30, c + 30, 3)) for _ in range(16)]
+    ne64, r64 = ne.double(), rays.double()
+
+    def loss_at(v):
+        with torch.no_grad():
+            return float((adjoint.detector_image(v, r64, spec, **kw, precision="f64") - target).pow(2).sum())
+    fd, ad = [], []
+    for v in vox:
+        eps = 1e-3 * float(ne64[v])
+        y = ne64.clone()
+        y[v] += eps
+        lp = loss_at(y)
+        y[v] -= 2 * eps
+        fd.append((lp - loss_at(y)) / (2 * eps))
+        ad.append(float(g32[v]))
+    fd, ad = np.array(fd), np.array(ad)
+    fms, bms = float(np.median(fwd_ms)), float(np.median(bwd_ms))
+    out = {"workload": "128^3 FP32 Kolmogorov grid, 1e6 rays (3 mm Gaussian beam), 400 RK4 steps, checkpoints "
+                       "every 20, 256^2 detector, 2-pixel Gaussian splat, L = ||I - I_target||^2",
+           "ray_steps": steps, "forward_ms": fms, "backward_ms": bms,
+           "forward_ray_steps_per_s": steps / (fms / 1e3), "backward_ray_steps_per_s": steps / (bms / 1e3),
+           "grad_vs_fd": {"voxels": len(vox), "max_abs_err_rel_to_max": float(np.abs(ad - fd).max() / np.abs(fd).max()),
+                          "fd": "central, eps = 1e-3 ne, FP64 forward"},
+           "timing": "CUDA events; forward = pack + Morton pre-pass + trace + splat; backward = loss grad + "
+                     "adjoint kernel + pack adjoint"}
+    del ne_t, ne, rays, target, g32
+    torch.cuda.empty_cache()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
 def run_sloth(args):
@@ -406,6 +475,11 @@ def run_sloth(args):
     if not args.no_serving:
         serve = run_serving(args)
 
+    # ---- adjoint: gradient of a detector-image loss -------------------------
+    adj = None
+    if not args.no_adjoint:
+        adj = run_adjoint(args)
+
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -443,6 +517,7 @@ def run_sloth(args):
             "fp64_port": fp64,
             "fp32_vs_fp64": acc,
             "serving": serve,
+            "adjoint": adj,
         }
         if fp64:
             line["fp64_port"]["speedup_of_fp32"] = value / world / fp64["value"]

@@ -242,6 +242,67 @@ int sloth_server_sync(SlothServer* s);
 int sloth_trace_f32_noalloc(const SlothGridDesc* g, const void* grid, const SlothTraceParams* p,
                             const float* rays, int64_t n, const SlothTraceOutputs* out, void* stream);
 
+/* ---- K4/K5: detector image and its adjoint --------------------------------
+ * No counterpart in the reference, which never differentiates. The forward
+ * model maps the packed grid to a detector image:
+ *   - fixed-step RK4 of the reference's ray equations (src/core/propagator.py
+ *     168-243: dv/dt = -(c^2/2) grad(ne/nc), trilinear gradient, fill 0
+ *     outside), at most n_steps steps of dtau, in the tracers' scaled scheme
+ *     but without face clipping. A ray stops early once it is outside the
+ *     grid on some axis and moving away from it along that axis.
+ *   - projection of the final ray on a straight line to the plane
+ *     `plane` along probing_axis (src/shared/propagation.py:92-134).
+ *   - a Gaussian splat into an n_px[0] x n_px[1] image covering
+ *     window = {u0, u1, v0, v1} (metres) on the two transverse axes in
+ *     ascending order (probing z: u = x, v = y; image[i][j], i along u).
+ *     A ray at pixel coordinates (a, b) (pixel i covers
+ *     [u0 + i du, u0 + (i+1) du)) adds g(i - a) g(j - b) / (2 pi s^2), with
+ *     g(d) = exp(-d^2 / 2s^2) times a taper that is 1 up to 3s and falls to 0
+ *     at 4s as a C2 smoothstep; s = sigma_px.
+ * The forward keeps each ray's state every ckpt_every steps in the workspace.
+ * The backward needs that workspace unchanged, and the same grid, params and n:
+ *   - it adds d L / d(packed grid) for the given d L / d image to grid_grad
+ *     (same layout as the packed grid; the entry point zeroes it first;
+ *     channel q stays 0);
+ *   - it recomputes each checkpoint segment and runs the discrete adjoint of
+ *     the RK4 steps in reverse.
+ * sloth_grid_pack_adjoint_* maps d L / d(packed grid) to d L / d ne through
+ * the transpose of sloth_grid_pack_*: ne_grad = ne_scale * (dq + sum over
+ * axes of the transposed difference stencil of the gradient channels).
+ * _f32: FP32 grid, rays, image and compensated FP32 state (as sloth_trace_f32);
+ * grid_grad accumulates with FP32 atomics. _f64: all FP64. */
+typedef struct SlothImageParams {
+    double  dtau;            /* RK4 step c*dt (m)                                  */
+    int32_t n_steps;         /* steps per ray, at most                             */
+    int32_t ckpt_every;      /* steps per checkpoint segment, 1 .. 32              */
+    int32_t probing_axis;    /* detector plane normal: 0, 1 or 2                   */
+    int32_t n_px[2];         /* image size (pixels) along the two transverse axes  */
+    int32_t reserved;        /* must be 0                                          */
+    double  plane;           /* detector plane position along probing_axis (m)     */
+    double  window[4];       /* u0, u1, v0, v1: detector extent (m)                */
+    double  sigma_px;        /* splat Gaussian sigma (pixels), 0 < sigma <= 8       */
+} SlothImageParams;
+
+size_t sloth_image_workspace_bytes(const SlothImageParams* p, int64_t n_rays);
+/* total_steps: device counter the forward adds every ray's step count to
+ * (the caller zeroes it; NULL skips). */
+int sloth_image_forward_f32(const SlothGridDesc* g, const void* grid, const SlothImageParams* p,
+                            const float* rays, int64_t n, float* image, unsigned long long* total_steps,
+                            void* workspace, size_t workspace_bytes, void* stream);
+int sloth_image_forward_f64(const SlothGridDesc* g, const void* grid, const SlothImageParams* p,
+                            const double* rays, int64_t n, double* image, unsigned long long* total_steps,
+                            void* workspace, size_t workspace_bytes, void* stream);
+int sloth_image_backward_f32(const SlothGridDesc* g, const void* grid, const SlothImageParams* p,
+                             int64_t n, const float* image_grad, void* grid_grad, void* workspace,
+                             size_t workspace_bytes, void* stream);
+int sloth_image_backward_f64(const SlothGridDesc* g, const void* grid, const SlothImageParams* p,
+                             int64_t n, const double* image_grad, void* grid_grad, void* workspace,
+                             size_t workspace_bytes, void* stream);
+int sloth_grid_pack_adjoint_f32(const SlothGridDesc* g, const void* grid_grad, double ne_scale,
+                                float* ne_grad, void* stream);
+int sloth_grid_pack_adjoint_f64(const SlothGridDesc* g, const void* grid_grad, double ne_scale,
+                                double* ne_grad, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

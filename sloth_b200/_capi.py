@@ -84,6 +84,12 @@ class SlothServerStats(Structure):
                 ("kernel_launches", ctypes.c_longlong)]
 
 
+class SlothImageParams(Structure):
+    _fields_ = [("dtau", c_double), ("n_steps", c_int32), ("ckpt_every", c_int32), ("probing_axis", c_int32),
+                ("n_px", c_int32 * 2), ("reserved", c_int32), ("plane", c_double), ("window", c_double * 4),
+                ("sigma_px", c_double)]
+
+
 SLOTH_JOB_PENDING, SLOTH_JOB_RUNNING, SLOTH_JOB_DONE, SLOTH_JOB_FETCHING, SLOTH_JOB_FETCHED = 0, 1, 2, 3, 4
 
 # name -> (restype, argtypes); every symbol include/sloth_b200.h declares.
@@ -114,6 +120,17 @@ _SIGNATURES = {
     "sloth_server_release": (c_int, [c_void_p, c_int]),
     "sloth_server_stats": (c_int, [c_void_p, POINTER(SlothServerStats)]),
     "sloth_server_sync": (c_int, [c_void_p]),
+    "sloth_image_workspace_bytes": (c_size_t, [POINTER(SlothImageParams), c_int64]),
+    "sloth_image_forward_f32": (c_int, [POINTER(SlothGridDesc), c_void_p, POINTER(SlothImageParams), c_void_p,
+                                        c_int64, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "sloth_image_forward_f64": (c_int, [POINTER(SlothGridDesc), c_void_p, POINTER(SlothImageParams), c_void_p,
+                                        c_int64, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "sloth_image_backward_f32": (c_int, [POINTER(SlothGridDesc), c_void_p, POINTER(SlothImageParams), c_int64,
+                                         c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "sloth_image_backward_f64": (c_int, [POINTER(SlothGridDesc), c_void_p, POINTER(SlothImageParams), c_int64,
+                                         c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "sloth_grid_pack_adjoint_f32": (c_int, [POINTER(SlothGridDesc), c_void_p, c_double, c_void_p, c_void_p]),
+    "sloth_grid_pack_adjoint_f64": (c_int, [POINTER(SlothGridDesc), c_void_p, c_double, c_void_p, c_void_p]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGNATURES)

@@ -1,0 +1,831 @@
+// Detector-image forward model and its adjoint: the gradient of a loss on a
+// synthetic detector image with respect to the density grid.
+//
+// No counterpart in the reference, which never differentiates. The model
+// differentiates the reference's ray equations (src/core/propagator.py:
+// 168-243, dr/dt = v, dv/dt = -(c^2/2) grad(ne/nc) from the precomputed
+// gradient grid through the trilinear interpolator, src/core/interpolator.py:
+// 79-104, fill 0 outside) through a detector image:
+//
+//   ne --pack (K1)--> (q, dq/du, dq/dv, dq/dw)
+//      --fixed-step RK4, at most n_steps steps--> final ray state
+//      --straight line to the detector plane--> (X, Y)
+//      --Gaussian splat--> image I
+//
+// RK4 is the tracer's scaled scheme (unit steps in grid cells) without face
+// clipping: every stage samples the interpolant with fill 0 outside, so a
+// ray's map is smooth except where a stage point crosses a grid face. A ray
+// stops early once it is outside the grid on some axis and moving away from
+// it along that axis: its remaining steps are straight lines, and the
+// projection to the detector plane (src/shared/propagation.py:92-134) gives
+// the same point from any point of that line.
+//
+// Splat: a ray at pixel coordinates (a, b) adds norm * g(i - a) * g(j - b)
+// to pixel (i, j), with g(d) = exp(-d^2 / (2 s^2)) * taper(|d| / s), taper = 1
+// up to 3 s and a C2 smoothstep from 1 to 0 between 3 s and 4 s, and norm =
+// 1 / (2 pi s^2). The taper keeps the splat twice differentiable with a
+// finite support of 4 s.
+//
+// Adjoint (backward): for each ray, d L / d(final state) from the image
+// gradient through the splat and the projection; then, segment by segment
+// from the last, the trajectory is recomputed from the segment's checkpoint
+// (the forward stores one every ckpt_every steps) and the discrete adjoint of
+// each RK4 step runs in reverse. Each stage's contribution to d L / d(grid
+// gradient channels) is accumulated in registers for the 8 corners of the
+// stage's cell and added to the grid-gradient buffer when the cell changes.
+// pack_adjoint_kernel maps d L / d(packed grid) through the transposed
+// difference stencil of K1 to d L / d ne.
+#include <cmath>
+
+#include "tracer.cuh"
+
+namespace sloth {
+
+constexpr int kAdjThreads = 256;
+constexpr int kMaxCkptEvery = 32;
+constexpr int kMaxTaps = 65;          // 2 * 4 * sigma + 1 pixels at sigma <= 8
+
+struct ImageArgs {
+    GridGeo geo;
+    const void* grid;
+    const void* rays;            // (6, n) of R, original order
+    long long n;
+    const unsigned* perm;        // slot -> ray id (bucket order)
+    double origin[3], w_of_v[3], inv_h[3];
+    double S[3];                 // -(dtau/h)^2 / 2
+    int n_steps, ckpt_every, n_seg;
+    int axis, t1, t2;
+    double plane;                // detector plane (cells along axis)
+    double px0[2], px_per_cell[2];
+    int npx[2];
+    int taps;                    // pixels per axis in a splat window
+    double sigma, radius, norm;  // pixels
+    void* ckpt;                  // [n_seg + 1][12 floats | 6 doubles][n]
+    int* nsteps;                 // steps taken, per slot
+    void* image;                 // forward: the image; backward: d L / d image
+    void* ggrad;                 // backward: d L / d(packed grid)
+    unsigned long long* total_steps;   // forward: steps of all rays are added here (may be null)
+};
+
+// ---------------------------------------------------------------------------
+// Ray state and checkpoints.
+// ---------------------------------------------------------------------------
+template <class P>
+struct MState {
+    typename P::Acc p[3], w[3];
+};
+
+// A checkpoint is 48 bytes per ray: FP32 stores the value and compensation of
+// each of the six sums, FP64 the six values; component-major for coalescing.
+template <class P>
+__device__ __forceinline__ void store_state(const ImageArgs& a, int k, long long slot, const MState<P>& r) {
+    if constexpr (sizeof(typename P::R) == 4) {
+        float* c = reinterpret_cast<float*>(a.ckpt) + (size_t)k * 12 * a.n + slot;
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            c[(2 * x) * a.n] = r.p[x].s;
+            c[(2 * x + 1) * a.n] = r.p[x].c;
+            c[(6 + 2 * x) * a.n] = r.w[x].s;
+            c[(7 + 2 * x) * a.n] = r.w[x].c;
+        }
+    } else {
+        double* c = reinterpret_cast<double*>(a.ckpt) + (size_t)k * 6 * a.n + slot;
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            c[x * a.n] = r.p[x].s;
+            c[(3 + x) * a.n] = r.w[x].s;
+        }
+    }
+}
+
+template <class P>
+__device__ __forceinline__ void load_state(const ImageArgs& a, int k, long long slot, MState<P>& r) {
+    if constexpr (sizeof(typename P::R) == 4) {
+        const float* c = reinterpret_cast<const float*>(a.ckpt) + (size_t)k * 12 * a.n + slot;
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            r.p[x].s = c[(2 * x) * a.n];
+            r.p[x].c = c[(2 * x + 1) * a.n];
+            r.w[x].s = c[(6 + 2 * x) * a.n];
+            r.w[x].c = c[(7 + 2 * x) * a.n];
+        }
+    } else {
+        const double* c = reinterpret_cast<const double*>(a.ckpt) + (size_t)k * 6 * a.n + slot;
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            r.p[x].s = c[x * a.n];
+            r.w[x].s = c[(3 + x) * a.n];
+        }
+    }
+}
+
+// Outside the grid on some axis and moving away from it along that axis (or
+// not finite): every later step is a straight line.
+template <class P>
+__device__ __forceinline__ bool ray_gone_model(const ImageArgs& a, const MState<P>& r) {
+    using R = typename P::R;
+    bool gone = false;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        const R p = r.p[x].val(), w = r.w[x].val();
+        gone |= (p < R(0) && w <= R(0)) || (p > lim_of<R>(a.geo, x) && w >= R(0)) || !(p == p) || !(w == w);
+    }
+    return gone;
+}
+
+// ---------------------------------------------------------------------------
+// The gradient channels of one cell as trilinear polynomials.
+// ---------------------------------------------------------------------------
+template <class P>
+struct GradCell {
+    unsigned base;
+    typename P::R t[3][8];
+};
+
+// Cell and in-cell coordinates of the point hi + lo (the tracer's split: the
+// cell from the rounded sum, the fractions from (hi - i) + lo). False when
+// the point is outside the grid (fill 0).
+template <class P>
+__device__ __forceinline__ bool locate(const GridGeo& g, const typename P::R (&hi)[3],
+                                       const typename P::R (&lo)[3], unsigned& base, typename P::R (&f)[3]) {
+    using R = typename P::R;
+    R p[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) p[x] = hi[x] + lo[x];
+    const bool in = (p[0] >= R(0)) & (p[0] <= lim_of<R>(g, 0)) & (p[1] >= R(0)) &
+                    (p[1] <= lim_of<R>(g, 1)) & (p[2] >= R(0)) & (p[2] <= lim_of<R>(g, 2));
+    if (!in) return false;
+    const int ix = min((int)p[0], g.n[0] - 2);
+    const int iy = min((int)p[1], g.n[1] - 2);
+    const int iz = min((int)p[2], g.n[2] - 2);
+    f[0] = (hi[0] - (R)ix) + lo[0];
+    f[1] = (hi[1] - (R)iy) + lo[1];
+    f[2] = (hi[2] - (R)iz) + lo[2];
+    base = (unsigned)ix * g.sx + (unsigned)iy * g.sy + (unsigned)iz;
+    return true;
+}
+
+template <class P>
+__device__ __forceinline__ void load_cell(const ImageArgs& a, unsigned b, GradCell<P>& cc) {
+    using R = typename P::R;
+    if (b == cc.base) return;
+    cc.base = b;
+    const GridGeo& g = a.geo;
+    const typename P::V v0 = P::load(a.grid, b), v1 = P::load(a.grid, b + 1u);
+    const typename P::V v2 = P::load(a.grid, b + g.sy), v3 = P::load(a.grid, b + g.sy + 1u);
+    const typename P::V v4 = P::load(a.grid, b + g.sx), v5 = P::load(a.grid, b + g.sx + 1u);
+    const typename P::V v6 = P::load(a.grid, b + g.sx + g.sy), v7 = P::load(a.grid, b + g.sx + g.sy + 1u);
+    poly_coeffs<R>(cc.t[0], v0.y, v1.y, v2.y, v3.y, v4.y, v5.y, v6.y, v7.y);
+    poly_coeffs<R>(cc.t[1], v0.z, v1.z, v2.z, v3.z, v4.z, v5.z, v6.z, v7.z);
+    poly_coeffs<R>(cc.t[2], v0.w, v1.w, v2.w, v3.w, v4.w, v5.w, v6.w, v7.w);
+}
+
+// Acceleration S * grad(q) at hi + lo (zero outside).
+template <class P>
+__device__ __forceinline__ void accel(const ImageArgs& a, const typename P::R (&hi)[3], const typename P::R (&lo)[3],
+                                      typename P::R (&A)[3], GradCell<P>& cc) {
+    using R = typename P::R;
+    unsigned b;
+    R f[3];
+    if (!locate<P>(a.geo, hi, lo, b, f)) {
+        A[0] = A[1] = A[2] = R(0);
+        return;
+    }
+    load_cell<P>(a, b, cc);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) A[k] = (R)a.S[k] * poly_eval<R>(cc.t[k], f[0], f[1], f[2]);
+}
+
+// One RK4 step (the tracer's rk4_step with phi = 1, without phase and depth):
+//   p' = p + w + (A1 + A2 + A3)/6,  w' = w + (A1 + 2A2 + 2A3 + A4)/6,
+//   stages at p, p + w/2, p + w/2 + A1/4, p + w + A2/2.
+template <class P>
+__device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, GradCell<P>& cc) {
+    using R = typename P::R;
+    R ph[3], pl[3], we[3], st[3], A1[3], A2[3], A3[3], A4[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        ph[x] = r.p[x].hi();
+        pl[x] = r.p[x].lo();
+        we[x] = r.w[x].val();
+    }
+    accel<P>(a, ph, pl, A1, cc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * we[x];
+    accel<P>(a, ph, st, A2, cc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * (we[x] + R(0.5) * A1[x]);
+    accel<P>(a, ph, st, A3, cc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + (we[x] + R(0.5) * A2[x]);
+    accel<P>(a, ph, st, A4, cc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        const R sA = (A1[x] + A2[x]) + A3[x];
+        const R sW = ((A1[x] + R(2) * A2[x]) + R(2) * A3[x]) + A4[x];
+        r.p[x].add(r.w[x].hi() + (r.w[x].lo() + sA * R(1.0 / 6.0)));
+        r.w[x].add(sW * R(1.0 / 6.0));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint of one RK4 step.
+// ---------------------------------------------------------------------------
+template <class P>
+struct CornerAcc {
+    unsigned base;               // cell of the pending sums (kNone: none)
+    typename P::R v[3][8];       // d L / d(channel k) at corner c
+};
+
+constexpr unsigned kNone = 0xffffffffu;
+
+template <class P>
+__device__ __forceinline__ void flush(const ImageArgs& a, CornerAcc<P>& acc) {
+    using R = typename P::R;
+    if (acc.base == kNone) return;
+    const GridGeo& g = a.geo;
+    const unsigned b = acc.base;
+    const unsigned off[8] = {b, b + 1u, b + g.sy, b + g.sy + 1u, b + g.sx, b + g.sx + 1u, b + g.sx + g.sy,
+                             b + g.sx + g.sy + 1u};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        if constexpr (sizeof(R) == 4) {
+            atomicAdd(reinterpret_cast<float4*>(a.ggrad) + off[c], make_float4(0.f, acc.v[0][c], acc.v[1][c], acc.v[2][c]));
+        } else {
+            double* d = reinterpret_cast<double*>(a.ggrad) + 4 * (size_t)off[c];
+            atomicAdd(d + 1, acc.v[0][c]);
+            atomicAdd(d + 2, acc.v[1][c]);
+            atomicAdd(d + 3, acc.v[2][c]);
+        }
+    }
+    acc.base = kNone;
+}
+
+// Stage adjoint: with Abar = d L / d(stage acceleration), adds
+// Abar_k * S_k * (corner weight) to the corners of the stage's cell and
+// returns q = J^T (S * Abar), J = d grad(q) / d p at the stage point.
+template <class P>
+__device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const typename P::R (&hi)[3],
+                                              const typename P::R (&lo)[3], const typename P::R (&Abar)[3],
+                                              typename P::R (&q)[3], GradCell<P>& cc, CornerAcc<P>& acc) {
+    using R = typename P::R;
+    unsigned b;
+    R f[3];
+    if (!locate<P>(a.geo, hi, lo, b, f)) {
+        q[0] = q[1] = q[2] = R(0);
+        return;
+    }
+    load_cell<P>(a, b, cc);
+    const R fx = f[0], fy = f[1], fz = f[2];
+    R gb[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) gb[k] = (R)a.S[k] * Abar[k];
+    // J^T gb: derivatives of the three trilinear polynomials
+    q[0] = q[1] = q[2] = R(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const R* t = cc.t[k];
+        const R dx = (t[1] + fy * t[4]) + fz * (t[5] + fy * t[7]);
+        const R dy = (t[2] + fx * t[4]) + fz * (t[6] + fx * t[7]);
+        const R dz = (t[3] + fx * t[5]) + fy * (t[6] + fx * t[7]);
+        q[0] += gb[k] * dx;
+        q[1] += gb[k] * dy;
+        q[2] += gb[k] * dz;
+    }
+    // corner weights, corner index 4*dx + 2*dy + dz
+    if (b != acc.base) {
+        flush<P>(a, acc);
+        acc.base = b;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc.v[k][c] = R(0);
+    }
+    const R ex = R(1) - fx, ey = R(1) - fy, ez = R(1) - fz;
+    const R w00 = ex * ey, w01 = ex * fy, w10 = fx * ey, w11 = fx * fy;
+    const R w[8] = {w00 * ez, w00 * fz, w01 * ez, w01 * fz, w10 * ez, w10 * fz, w11 * ez, w11 * fz};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc.v[k][c] += gb[k] * w[c];
+}
+
+// Reverse of model_step from the step's input state r: (lp, lw) = adjoint of
+// the output (p', w') on entry, of the input (p, w) on return.
+template <class P>
+__device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const MState<P>& r, typename P::R (&lp)[3],
+                                                   typename P::R (&lw)[3], GradCell<P>& cc, CornerAcc<P>& acc) {
+    using R = typename P::R;
+    R ph[3], pl[3], we[3], st[3], A1[3], A2[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        ph[x] = r.p[x].hi();
+        pl[x] = r.p[x].lo();
+        we[x] = r.w[x].val();
+    }
+    // stage accelerations that place the later stages
+    accel<P>(a, ph, pl, A1, cc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * we[x];
+    accel<P>(a, ph, st, A2, cc);
+    R a1[3], a2[3], a3[3], a4[3], pb[3], wb[3], q[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        a1[x] = (lp[x] + lw[x]) * R(1.0 / 6.0);
+        a2[x] = lp[x] * R(1.0 / 6.0) + lw[x] * R(1.0 / 3.0);
+        a3[x] = a2[x];
+        a4[x] = lw[x] * R(1.0 / 6.0);
+        pb[x] = lp[x];
+        wb[x] = lp[x] + lw[x];
+    }
+    // stage 4 at p + w + A2/2
+#pragma unroll
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + (we[x] + R(0.5) * A2[x]);
+    stage_adjoint<P>(a, ph, st, a4, q, cc, acc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        pb[x] += q[x];
+        wb[x] += q[x];
+        a2[x] += R(0.5) * q[x];
+    }
+    // stage 3 at p + w/2 + A1/4
+#pragma unroll
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * (we[x] + R(0.5) * A1[x]);
+    stage_adjoint<P>(a, ph, st, a3, q, cc, acc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        pb[x] += q[x];
+        wb[x] += R(0.5) * q[x];
+        a1[x] += R(0.25) * q[x];
+    }
+    // stage 2 at p + w/2
+#pragma unroll
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * we[x];
+    stage_adjoint<P>(a, ph, st, a2, q, cc, acc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        pb[x] += q[x];
+        wb[x] += R(0.5) * q[x];
+    }
+    // stage 1 at p
+    stage_adjoint<P>(a, ph, pl, a1, q, cc, acc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        lp[x] = pb[x] + q[x];
+        lw[x] = wb[x];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Detector projection and splat.
+// ---------------------------------------------------------------------------
+
+// Splat profile g(d) and its derivative dg/dd (d and s in pixels).
+template <class R>
+__device__ __forceinline__ R splat_g(R d, R s, R& dg) {
+    const R u = fabs(d) / s;
+    if (u >= R(4)) {
+        dg = R(0);
+        return R(0);
+    }
+    R e;
+    if constexpr (sizeof(R) == 4) e = expf(R(-0.5) * u * u);
+    else e = exp(R(-0.5) * u * u);
+    R t = R(1), dt = R(0);
+    if (u > R(3)) {
+        const R x = u - R(3);
+        t = R(1) - x * x * x * (R(10) + x * (R(-15) + x * R(6)));
+        dt = R(-30) * x * x * (R(1) - x) * (R(1) - x);
+    }
+    // d/dd [e(u) t(u)] with u = |d|/s
+    const R sgn = d < R(0) ? R(-1) : R(1);
+    dg = (e * (-u * t + dt)) * sgn / s;
+    return e * t;
+}
+
+// Detector coordinates (pixels) of a final state; false if the ray never
+// meets the plane or is not finite.
+template <class P>
+__device__ __forceinline__ bool detector_point(const ImageArgs& a, const MState<P>& r, double& pa, double& pb,
+                                               double& t, double (&p)[3], double (&w)[3]) {
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        p[x] = r.p[x].vald();
+        w[x] = r.w[x].vald();
+    }
+    const double wa = a.axis == 0 ? w[0] : (a.axis == 1 ? w[1] : w[2]);
+    const double pax = a.axis == 0 ? p[0] : (a.axis == 1 ? p[1] : p[2]);
+    if (!(wa != 0.0)) return false;
+    t = (a.plane - pax) / wa;
+    const double X = p[a.t1] + t * w[a.t1];
+    const double Y = p[a.t2] + t * w[a.t2];
+    pa = a.px0[0] + a.px_per_cell[0] * X;
+    pb = a.px0[1] + a.px_per_cell[1] * Y;
+    return isfinite(pa) && isfinite(pb) && fabs(pa) < 1e9 && fabs(pb) < 1e9;
+}
+
+template <class P>
+__device__ __forceinline__ void splat(const ImageArgs& a, double pa, double pb) {
+    using R = typename P::R;
+    const int i0 = (int)floor(pa - a.radius) + 1;
+    const int j0 = (int)floor(pb - a.radius) + 1;
+    const R s = (R)a.sigma;
+    R gy[kMaxTaps];
+    for (int j = 0; j < a.taps; ++j) {
+        R dg;
+        gy[j] = splat_g<R>((R)((double)(j0 + j) - pb), s, dg);
+    }
+    R* img = reinterpret_cast<R*>(a.image);
+    for (int i = 0; i < a.taps; ++i) {
+        const int ii = i0 + i;
+        if (ii < 0 || ii >= a.npx[0]) continue;
+        R dg;
+        const R gx = splat_g<R>((R)((double)ii - pa), s, dg) * (R)a.norm;
+        if (gx == R(0)) continue;
+        for (int j = 0; j < a.taps; ++j) {
+            const int jj = j0 + j;
+            if (jj < 0 || jj >= a.npx[1] || gy[j] == R(0)) continue;
+            atomicAdd(img + (size_t)ii * a.npx[1] + jj, gx * gy[j]);
+        }
+    }
+}
+
+// d L / d(pixel coordinates) from the image gradient.
+template <class P>
+__device__ __forceinline__ void splat_adjoint(const ImageArgs& a, double pa, double pb, double& ga, double& gb) {
+    using R = typename P::R;
+    const int i0 = (int)floor(pa - a.radius) + 1;
+    const int j0 = (int)floor(pb - a.radius) + 1;
+    const R s = (R)a.sigma;
+    R gy[kMaxTaps], dgy[kMaxTaps];
+    for (int j = 0; j < a.taps; ++j) gy[j] = splat_g<R>((R)((double)(j0 + j) - pb), s, dgy[j]);
+    const R* gi = reinterpret_cast<const R*>(a.image);
+    R sa = R(0), sb = R(0);
+    for (int i = 0; i < a.taps; ++i) {
+        const int ii = i0 + i;
+        if (ii < 0 || ii >= a.npx[0]) continue;
+        R dgx;
+        const R gx = splat_g<R>((R)((double)ii - pa), s, dgx);
+        if (gx == R(0) && dgx == R(0)) continue;
+        R r0 = R(0), r1 = R(0);
+        for (int j = 0; j < a.taps; ++j) {
+            const int jj = j0 + j;
+            if (jj < 0 || jj >= a.npx[1]) continue;
+            const R v = gi[(size_t)ii * a.npx[1] + jj];
+            r0 += v * gy[j];
+            r1 += v * dgy[j];
+        }
+        // d/da g(i - a) = -g'(i - a)
+        sa -= dgx * r0;
+        sb -= gx * r1;
+    }
+    ga = (double)sa * a.norm;
+    gb = (double)sb * a.norm;
+}
+
+// ---------------------------------------------------------------------------
+// Kernels.
+// ---------------------------------------------------------------------------
+template <class P>
+__global__ void __launch_bounds__(kAdjThreads) image_forward_kernel(const __grid_constant__ ImageArgs a) {
+    using R = typename P::R;
+    __shared__ unsigned long long s_steps;
+    if (threadIdx.x == 0) s_steps = 0;
+    __syncthreads();
+    const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int t = 0;
+    if (slot < a.n) {
+        const unsigned id = a.perm[slot];
+        const R* rays = reinterpret_cast<const R*>(a.rays);
+        MState<P> r;
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            r.p[x].set(((double)rays[x * a.n + id] - a.origin[x]) * a.inv_h[x]);
+            r.w[x].set((double)rays[(3 + x) * a.n + id] * a.w_of_v[x]);
+        }
+        GradCell<P> cc;
+        cc.base = kNone;
+        for (; t < a.n_steps; ++t) {
+            if (ray_gone_model<P>(a, r)) break;
+            if (t % a.ckpt_every == 0) store_state<P>(a, t / a.ckpt_every, slot, r);
+            model_step<P>(a, r, cc);
+        }
+        store_state<P>(a, a.n_seg, slot, r);
+        a.nsteps[slot] = t;
+        double pa, pb, tt, p[3], w[3];
+        if (detector_point<P>(a, r, pa, pb, tt, p, w)) splat<P>(a, pa, pb);
+    }
+    block_add((unsigned long long)t, &s_steps, a.total_steps);
+}
+
+template <class P>
+__global__ void __launch_bounds__(kAdjThreads) image_backward_kernel(const __grid_constant__ ImageArgs a) {
+    using R = typename P::R;
+    const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= a.n) return;
+    MState<P> r;
+    load_state<P>(a, a.n_seg, slot, r);
+    double pa, pb, t, p[3], w[3];
+    if (!detector_point<P>(a, r, pa, pb, t, p, w)) return;
+    double ga, gb;
+    splat_adjoint<P>(a, pa, pb, ga, gb);
+    // projection X = p1 + t w1, Y = p2 + t w2, t = (plane - pa) / wa
+    const double Xb = ga * a.px_per_cell[0], Yb = gb * a.px_per_cell[1];
+    const double wa = a.axis == 0 ? w[0] : (a.axis == 1 ? w[1] : w[2]);
+    const double tb = Xb * w[a.t1] + Yb * w[a.t2];
+    double lpd[3] = {0.0, 0.0, 0.0}, lwd[3] = {0.0, 0.0, 0.0};
+    lpd[a.t1] = Xb;
+    lwd[a.t1] = Xb * t;
+    lpd[a.t2] = Yb;
+    lwd[a.t2] = Yb * t;
+    lpd[a.axis] = -tb / wa;
+    lwd[a.axis] = -tb * t / wa;
+    R lp[3], lw[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        lp[x] = (R)lpd[x];
+        lw[x] = (R)lwd[x];
+    }
+    if (lp[0] == R(0) && lp[1] == R(0) && lp[2] == R(0) && lw[0] == R(0) && lw[1] == R(0) && lw[2] == R(0))
+        return;
+    const int T = a.nsteps[slot];
+    GradCell<P> cc;
+    cc.base = kNone;
+    CornerAcc<P> acc;
+    acc.base = kNone;
+    MState<P> seg[kMaxCkptEvery];
+    for (int s = (T + a.ckpt_every - 1) / a.ckpt_every - 1; s >= 0; --s) {
+        load_state<P>(a, s, slot, r);
+        const int j0 = s * a.ckpt_every;
+        const int m = min(a.ckpt_every, T - j0);
+        for (int j = 0; j < m; ++j) {
+            seg[j] = r;
+            if (j + 1 < m) model_step<P>(a, r, cc);
+        }
+        for (int j = m - 1; j >= 0; --j) model_step_adjoint<P>(a, seg[j], lp, lw, cc, acc);
+    }
+    flush<P>(a, acc);
+}
+
+// d L / d ne from d L / d(packed grid): the transpose of K1's per-axis
+// stencil (one-sided differences on the faces, central inside), times
+// ne_scale. Gathers from the 6 neighbours; no atomics.
+template <class P>
+__device__ __forceinline__ void load_gg(const void* gg, size_t i, double (&v)[4]) {
+    if constexpr (sizeof(typename P::R) == 4) {
+        const float4 x = reinterpret_cast<const float4*>(gg)[i];
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    } else {
+        const double* d = reinterpret_cast<const double*>(gg) + 4 * i;
+        v[0] = d[0]; v[1] = d[1]; v[2] = d[2]; v[3] = d[3];
+    }
+}
+
+// Transpose of one axis' stencil at index j of n: sum over the differences
+// D[i] that use q[j] of d D[i] / d q[j] * Dbar[i], where Dbar[i] is channel
+// `ch` of the neighbour at offset (i - j) * stride.
+template <class P>
+__device__ __forceinline__ double stencil_t(const void* gg, size_t v, int j, int n, size_t stride, int ch) {
+    double r = 0.0, x[4];
+    if (j >= 1) {          // D[j-1] holds +q[j] with weight 1 (face j-1 == 0) or 1/2
+        load_gg<P>(gg, v - stride, x);
+        r += (j - 1 == 0 ? 1.0 : 0.5) * x[ch];
+    }
+    if (j <= n - 2) {      // D[j+1] holds -q[j] with weight 1 (face j+1 == n-1) or 1/2
+        load_gg<P>(gg, v + stride, x);
+        r -= (j + 1 == n - 1 ? 1.0 : 0.5) * x[ch];
+    }
+    if (j == 0 || j == n - 1) {   // the one-sided differences on the faces use q[j] itself
+        load_gg<P>(gg, v, x);
+        r += (j == 0 ? -1.0 : 1.0) * x[ch];
+    }
+    return r;
+}
+
+template <class P, class Out>
+__global__ void __launch_bounds__(256) pack_adjoint_kernel(const void* __restrict__ gg, Out* __restrict__ out,
+                                                           GridGeo g, double scale, long long total) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < total; v += stride) {
+        const int k = (int)(v % g.n[2]);
+        const long long t = v / g.n[2];
+        const int j = (int)(t % g.n[1]);
+        const int i = (int)(t / g.n[1]);
+        const size_t vi = (size_t)v;
+        double self[4];
+        load_gg<P>(gg, vi, self);
+        double r = self[0];
+        r += stencil_t<P>(gg, vi, i, g.n[0], g.sx, 1);
+        r += stencil_t<P>(gg, vi, j, g.n[1], g.sy, 2);
+        r += stencil_t<P>(gg, vi, k, g.n[2], 1, 3);
+        out[vi] = (Out)(r * scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+static int image_n_seg(const SlothImageParams* p) { return (p->n_steps + p->ckpt_every - 1) / p->ckpt_every; }
+
+static size_t image_ws_bytes(const SlothImageParams* p, long long n) {
+    const size_t nn = (size_t)(n > 0 ? n : 1);
+    return workspace_bytes(n) + align256((size_t)(image_n_seg(p) + 1) * 48u * nn) + align256(4u * nn);
+}
+
+static int check_image_params(const SlothGridDesc* g, const SlothImageParams* p, int64_t n) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (!p) return SLOTH_ERR_NULL_POINTER;
+    if (n < 0) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (n > 2147483647LL) return SLOTH_ERR_TOO_LARGE;
+    if (p->reserved != 0 || !(p->dtau > 0.0) || !std::isfinite(p->dtau)) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (p->n_steps < 1 || p->n_steps > 1000000) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (p->ckpt_every < 1 || p->ckpt_every > kMaxCkptEvery) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (p->probing_axis < 0 || p->probing_axis > 2) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (p->n_px[0] < 1 || p->n_px[1] < 1 || p->n_px[0] > 16384 || p->n_px[1] > 16384) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (!(p->sigma_px > 0.0) || !(p->sigma_px <= 8.0)) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (!std::isfinite(p->plane)) return SLOTH_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 4; ++k)
+        if (!std::isfinite(p->window[k])) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (!(p->window[1] > p->window[0]) || !(p->window[3] > p->window[2])) return SLOTH_ERR_INVALID_ARGUMENT;
+    return SLOTH_OK;
+}
+
+static void fill_image_args(ImageArgs& a, const SlothGridDesc* g, const void* grid, const SlothImageParams* p,
+                            const void* rays, long long n, const unsigned* perm, void* ckpt, int* nsteps) {
+    a.geo = make_geo(g);
+    a.grid = grid;
+    a.rays = rays;
+    a.n = n;
+    a.perm = perm;
+    for (int k = 0; k < 3; ++k) {
+        const double h = g->spacing[k];
+        a.origin[k] = g->origin[k];
+        a.inv_h[k] = 1.0 / h;
+        a.w_of_v[k] = (p->dtau / h) / kC;
+        a.S[k] = -0.5 * (p->dtau / h) * (p->dtau / h);
+    }
+    a.n_steps = p->n_steps;
+    a.ckpt_every = p->ckpt_every;
+    a.n_seg = image_n_seg(p);
+    a.axis = p->probing_axis;
+    a.t1 = a.axis == 0 ? 1 : 0;
+    a.t2 = a.axis == 2 ? 1 : 2;
+    a.plane = (p->plane - g->origin[a.axis]) / g->spacing[a.axis];
+    const int tr[2] = {a.t1, a.t2};
+    for (int d = 0; d < 2; ++d) {
+        const double lo = p->window[2 * d], hi = p->window[2 * d + 1];
+        const double pix = (hi - lo) / p->n_px[d];
+        a.px_per_cell[d] = g->spacing[tr[d]] / pix;
+        a.px0[d] = (g->origin[tr[d]] - lo) / pix - 0.5;
+        a.npx[d] = p->n_px[d];
+    }
+    a.sigma = p->sigma_px;
+    a.radius = 4.0 * p->sigma_px;
+    a.taps = 2 * (int)ceil(a.radius) + 1;
+    a.norm = 1.0 / (2.0 * 3.141592653589793 * p->sigma_px * p->sigma_px);
+    a.ckpt = ckpt;
+    a.nsteps = nsteps;
+    a.image = nullptr;
+    a.ggrad = nullptr;
+    a.total_steps = nullptr;
+}
+
+struct ImageWs {
+    unsigned *hist, *keys, *perm, *skeys;
+    void* ckpt;
+    int* nsteps;
+};
+
+static ImageWs carve(void* ws, const SlothImageParams* p, long long n) {
+    ImageWs w;
+    char* base = reinterpret_cast<char*>(ws);
+    const size_t a = align256((size_t)(n > 0 ? n : 1) * 4u);
+    w.hist = reinterpret_cast<unsigned*>(base + kHeaderBytes);
+    w.keys = reinterpret_cast<unsigned*>(base + kHeaderBytes + kHistBytes);
+    w.perm = reinterpret_cast<unsigned*>(base + kHeaderBytes + kHistBytes + a);
+    w.skeys = reinterpret_cast<unsigned*>(base + kHeaderBytes + kHistBytes + 2 * a);
+    char* c = base + workspace_bytes(n);
+    w.ckpt = c;
+    w.nsteps = reinterpret_cast<int*>(c + align256((size_t)(image_n_seg(p) + 1) * 48u * (size_t)(n > 0 ? n : 1)));
+    return w;
+}
+
+template <class P>
+static int image_forward_impl(const SlothGridDesc* g, const void* grid, const SlothImageParams* p,
+                              const typename P::R* rays, int64_t n, typename P::R* image,
+                              unsigned long long* total_steps, void* ws, size_t ws_bytes, void* stream) {
+    int rc = check_image_params(g, p, n);
+    if (rc) return rc;
+    if (!grid || !image || !ws || (n > 0 && !rays)) return SLOTH_ERR_NULL_POINTER;
+    if (((uintptr_t)grid & 15u) || ((uintptr_t)ws & 255u) || ((uintptr_t)image & (sizeof(typename P::R) - 1)) ||
+        ((uintptr_t)rays & (sizeof(typename P::R) - 1)))
+        return SLOTH_ERR_MISALIGNED;
+    if (ws_bytes < image_ws_bytes(p, n)) return SLOTH_ERR_WORKSPACE_TOO_SMALL;
+    int sms = 148;
+    if ((rc = device_sm_count(&sms)) != SLOTH_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(image, 0, sizeof(typename P::R) * (size_t)p->n_px[0] * p->n_px[1], s);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (n == 0) return SLOTH_OK;
+    ImageWs w = carve(ws, p, n);
+    const int bbits = bucket_bits_for(n);
+    if ((e = cudaMemsetAsync(w.hist, 0, (size_t)4 << bbits, s)) != cudaSuccess) return cuda_status(e);
+    rc = launch_prepass<typename P::R>(g, p->probing_axis, rays, n, bbits, w.keys, w.hist, w.perm, w.skeys, sms, s);
+    if (rc) return rc;
+    ImageArgs a;
+    fill_image_args(a, g, grid, p, rays, n, w.perm, w.ckpt, w.nsteps);
+    a.image = image;
+    a.total_steps = total_steps;
+    image_forward_kernel<P><<<(unsigned)((n + kAdjThreads - 1) / kAdjThreads), kAdjThreads, 0, s>>>(a);
+    note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+template <class P>
+static int image_backward_impl(const SlothGridDesc* g, const void* grid, const SlothImageParams* p, int64_t n,
+                               const typename P::R* image_grad, void* grid_grad, void* ws, size_t ws_bytes,
+                               void* stream) {
+    int rc = check_image_params(g, p, n);
+    if (rc) return rc;
+    if (!grid || !image_grad || !grid_grad || !ws) return SLOTH_ERR_NULL_POINTER;
+    if (((uintptr_t)grid & 15u) || ((uintptr_t)grid_grad & 15u) || ((uintptr_t)ws & 255u) ||
+        ((uintptr_t)image_grad & (sizeof(typename P::R) - 1)))
+        return SLOTH_ERR_MISALIGNED;
+    if (ws_bytes < image_ws_bytes(p, n)) return SLOTH_ERR_WORKSPACE_TOO_SMALL;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t vox = (size_t)g->n[0] * g->n[1] * g->n[2];
+    cudaError_t e = cudaMemsetAsync(grid_grad, 0, vox * 4 * sizeof(typename P::R), s);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (n == 0) return SLOTH_OK;
+    ImageWs w = carve(ws, p, n);
+    ImageArgs a;
+    fill_image_args(a, g, grid, p, nullptr, n, w.perm, w.ckpt, w.nsteps);
+    a.image = const_cast<typename P::R*>(image_grad);
+    a.ggrad = grid_grad;
+    image_backward_kernel<P><<<(unsigned)((n + kAdjThreads - 1) / kAdjThreads), kAdjThreads, 0, s>>>(a);
+    note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+template <class P, class Out>
+static int pack_adjoint_impl(const SlothGridDesc* g, const void* grid_grad, double ne_scale, Out* ne_grad,
+                             void* stream) {
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (!grid_grad || !ne_grad) return SLOTH_ERR_NULL_POINTER;
+    if (!(ne_scale > 0.0) || !std::isfinite(ne_scale)) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (((uintptr_t)grid_grad & 15u) || ((uintptr_t)ne_grad & (sizeof(Out) - 1))) return SLOTH_ERR_MISALIGNED;
+    int sms = 148;
+    if ((rc = device_sm_count(&sms)) != SLOTH_OK) return rc;
+    const long long total = (long long)g->n[0] * g->n[1] * g->n[2];
+    long long blocks = (total + 255) / 256;
+    if (blocks > (long long)sms * 16) blocks = (long long)sms * 16;
+    pack_adjoint_kernel<P, Out><<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(grid_grad, ne_grad,
+                                                                                   make_geo(g), ne_scale, total);
+    note_launch();
+    return cuda_status(cudaGetLastError());
+}
+
+}  // namespace sloth
+
+extern "C" {
+
+size_t sloth_image_workspace_bytes(const SlothImageParams* p, int64_t n) {
+    if (!p || p->ckpt_every < 1 || p->n_steps < 1 || n < 0) return 0;
+    return sloth::image_ws_bytes(p, n);
+}
+
+int sloth_image_forward_f32(const SlothGridDesc* g, const void* grid, const SlothImageParams* p, const float* rays,
+                            int64_t n, float* image, unsigned long long* total_steps, void* ws, size_t ws_bytes,
+                            void* stream) {
+    return sloth::image_forward_impl<sloth::PolF32>(g, grid, p, rays, n, image, total_steps, ws, ws_bytes, stream);
+}
+
+int sloth_image_forward_f64(const SlothGridDesc* g, const void* grid, const SlothImageParams* p, const double* rays,
+                            int64_t n, double* image, unsigned long long* total_steps, void* ws, size_t ws_bytes,
+                            void* stream) {
+    return sloth::image_forward_impl<sloth::PolF64>(g, grid, p, rays, n, image, total_steps, ws, ws_bytes, stream);
+}
+
+int sloth_image_backward_f32(const SlothGridDesc* g, const void* grid, const SlothImageParams* p, int64_t n,
+                             const float* image_grad, void* grid_grad, void* ws, size_t ws_bytes, void* stream) {
+    return sloth::image_backward_impl<sloth::PolF32>(g, grid, p, n, image_grad, grid_grad, ws, ws_bytes, stream);
+}
+
+int sloth_image_backward_f64(const SlothGridDesc* g, const void* grid, const SlothImageParams* p, int64_t n,
+                             const double* image_grad, void* grid_grad, void* ws, size_t ws_bytes, void* stream) {
+    return sloth::image_backward_impl<sloth::PolF64>(g, grid, p, n, image_grad, grid_grad, ws, ws_bytes, stream);
+}
+
+int sloth_grid_pack_adjoint_f32(const SlothGridDesc* g, const void* grid_grad, double ne_scale, float* ne_grad,
+                                void* stream) {
+    return sloth::pack_adjoint_impl<sloth::PolF32, float>(g, grid_grad, ne_scale, ne_grad, stream);
+}
+
+int sloth_grid_pack_adjoint_f64(const SlothGridDesc* g, const void* grid_grad, double ne_scale, double* ne_grad,
+                                void* stream) {
+    return sloth::pack_adjoint_impl<sloth::PolF64, double>(g, grid_grad, ne_scale, ne_grad, stream);
+}
+
+}  // extern "C"
