@@ -303,6 +303,65 @@ int sloth_grid_pack_adjoint_f32(const SlothGridDesc* g, const void* grid_grad, d
 int sloth_grid_pack_adjoint_f64(const SlothGridDesc* g, const void* grid_grad, double ne_scale,
                                 double* ne_grad, void* stream);
 
+/* ---- K6: ray-transfer-matrix diagnostics ----------------------------------
+ * Replaces the optics and histogram of src/processing/diagnostics.py
+ * (lens, travel, the apertures and stops, knife_edge, the lens_cutoff
+ * prefilter, Diagnostic.histogram; :16-128, :176-268) on Jones vectors
+ * (4, N) = (x, theta, y, phi), e.g. a trace's last save. Per ray:
+ *   1. if prefilter: keep only rays with sqrt((L tan theta + x)^2 +
+ *      (L tan phi + y)^2) <= R, on the input as given;
+ *   2. rows 0 and 2 times pos_scale (1e3 for the reference's m -> mm),
+ *      rounded in the input's precision;
+ *   3. the optics in order, in FP64 (see SLOTH_OPTIC_*). Travel and lens
+ *      are 4x4 matrix products in the reference, so a NaN in any component
+ *      makes all four NaN. The stops set all four to NaN;
+ *   4. if ccd_clip: keep |x| <= ccd_half[0] and |y| <= ccd_half[1];
+ *   5. if hist != NULL: add the ray's weight (1 if weights is NULL) to
+ *      hist[iy][ix] (ny x nx, doubles; the entry point adds, the caller
+ *      zeroes). The bins are numpy.histogram2d's over x_range x y_range:
+ *      numpy's linspace edges, the upper edge in the last bin, NaN and
+ *      out-of-range values dropped. The reference's H is this transposed
+ *      layout.
+ * rays_out (4, N) doubles (optional) receives the rays after step 3, with
+ * NaN for rejected rays. kept (N bytes, optional) receives 1 for rays the
+ * prefilter keeps. */
+#define SLOTH_OPTIC_TRAVEL             1  /* a = distance: x += a*theta, y += a*phi          */
+#define SLOTH_OPTIC_LENS               2  /* a = f1, b = f2: theta -= x/f1, phi -= y/f2      */
+#define SLOTH_OPTIC_CIRCULAR_APERTURE  3  /* a = R: rejects x^2 + y^2 > R^2                  */
+#define SLOTH_OPTIC_CIRCULAR_STOP      4  /* a = R: rejects x^2 + y^2 < R^2                  */
+#define SLOTH_OPTIC_RECT_APERTURE      5  /* a = Lx, b = Ly: rejects x^2 > Lx^2 AND y^2 > Ly^2
+                                             (the reference's rect_aperture, as written)     */
+#define SLOTH_OPTIC_KNIFE_EDGE         6  /* axis = 0 (x) or 2 (y), a = offset, b = direction:
+                                             rejects v > a if b > 0, v < a if b < 0          */
+#define SLOTH_OPTIC_ANNULAR_STOP       7  /* a = R1, b = R2: rejects R1^2 < r^2 < R2^2        */
+#define SLOTH_MAX_OPTICS 32
+
+typedef struct SlothOptic {
+    int32_t kind;            /* SLOTH_OPTIC_*                                      */
+    int32_t axis;            /* knife edge only                                    */
+    double  a, b;
+} SlothOptic;
+
+typedef struct SlothDetectorParams {
+    int32_t nx, ny;          /* histogram bins along x (row 0) and y (row 2)        */
+    double  x_range[2];      /* histogram range along x                            */
+    double  y_range[2];
+    double  pos_scale;       /* factor on rows 0 and 2 before the optics           */
+    int32_t prefilter;       /* 1: lens_cutoff prefilter with prefilter_L, _R      */
+    int32_t ccd_clip;        /* 1: clip to |x| <= ccd_half[0], |y| <= ccd_half[1]  */
+    double  prefilter_L, prefilter_R;
+    double  ccd_half[2];
+    int32_t reserved;        /* must be 0                                          */
+    int32_t reserved2;
+} SlothDetectorParams;
+
+int sloth_optics_f32(const float* rays, int64_t n, const float* weights, const SlothOptic* optics,
+                     int32_t n_optics, const SlothDetectorParams* d, double* hist, double* rays_out,
+                     uint8_t* kept, void* stream);
+int sloth_optics_f64(const double* rays, int64_t n, const double* weights, const SlothOptic* optics,
+                     int32_t n_optics, const SlothDetectorParams* d, double* hist, double* rays_out,
+                     uint8_t* kept, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

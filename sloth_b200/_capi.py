@@ -84,6 +84,22 @@ class SlothServerStats(Structure):
                 ("kernel_launches", ctypes.c_longlong)]
 
 
+class SlothOptic(Structure):
+    _fields_ = [("kind", c_int32), ("axis", c_int32), ("a", c_double), ("b", c_double)]
+
+
+class SlothDetectorParams(Structure):
+    _fields_ = [("nx", c_int32), ("ny", c_int32), ("x_range", c_double * 2), ("y_range", c_double * 2),
+                ("pos_scale", c_double), ("prefilter", c_int32), ("ccd_clip", c_int32), ("prefilter_L", c_double),
+                ("prefilter_R", c_double), ("ccd_half", c_double * 2), ("reserved", c_int32),
+                ("reserved2", c_int32)]
+
+
+(SLOTH_OPTIC_TRAVEL, SLOTH_OPTIC_LENS, SLOTH_OPTIC_CIRCULAR_APERTURE, SLOTH_OPTIC_CIRCULAR_STOP,
+ SLOTH_OPTIC_RECT_APERTURE, SLOTH_OPTIC_KNIFE_EDGE, SLOTH_OPTIC_ANNULAR_STOP) = range(1, 8)
+SLOTH_MAX_OPTICS = 32
+
+
 class SlothImageParams(Structure):
     _fields_ = [("dtau", c_double), ("n_steps", c_int32), ("ckpt_every", c_int32), ("probing_axis", c_int32),
                 ("n_px", c_int32 * 2), ("reserved", c_int32), ("plane", c_double), ("window", c_double * 4),
@@ -131,6 +147,10 @@ _SIGNATURES = {
                                          c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "sloth_grid_pack_adjoint_f32": (c_int, [POINTER(SlothGridDesc), c_void_p, c_double, c_void_p, c_void_p]),
     "sloth_grid_pack_adjoint_f64": (c_int, [POINTER(SlothGridDesc), c_void_p, c_double, c_void_p, c_void_p]),
+    "sloth_optics_f32": (c_int, [c_void_p, c_int64, c_void_p, POINTER(SlothOptic), c_int32,
+                                 POINTER(SlothDetectorParams), c_void_p, c_void_p, c_void_p, c_void_p]),
+    "sloth_optics_f64": (c_int, [c_void_p, c_int64, c_void_p, POINTER(SlothOptic), c_int32,
+                                 POINTER(SlothDetectorParams), c_void_p, c_void_p, c_void_p, c_void_p]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGNATURES)

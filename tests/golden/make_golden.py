@@ -12,8 +12,12 @@ Everything else -- precompute_gradients, kappa_inv_brems, the trilinear
 interpolator, dsdt, ray_to_Jonesvector, Beam, trace_and_save_depths, solve --
 is the reference's own code, unmodified, read from its source tree.
 
+The diagnostics module also imports matplotlib and sympy, which are not
+installed either; only their names are needed (`Matrix` is used by the
+reference's unused `ray` helper), so they are empty stand-ins.
+
 Usage (in a container that has the reference at /root/reference):
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py [/path/to/reference] [--only=diagnostics]
 Writes tests/golden/*.npz. The fixtures are committed; nothing on a GPU box
 or in the tests reads the reference tree.
 """
@@ -25,7 +29,9 @@ import types
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+_POS = [a for a in sys.argv[1:] if not a.startswith("--")]
+REF = _POS[0] if _POS else "/root/reference"
+ONLY = next((a.split("=", 1)[1] for a in sys.argv[1:] if a.startswith("--only=")), None)
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -182,6 +188,9 @@ def _install_stubs():
 def main():
     _install_stubs()
     sys.path.insert(0, os.path.join(REF, "src"))
+    if ONLY == "diagnostics":
+        diagnostics_golden()
+        return
     import core.interpolator as ci           # noqa: E402
     import core.propagator as cp             # noqa: E402
     import shared.propagation as sp          # noqa: E402
@@ -259,6 +268,7 @@ def main():
     # 7. trace_and_save_depths end to end (reference test cases) and solve()
     tr = _trace_cases(cp, c)
     np.savez(os.path.join(OUT, "trace_cases.npz"), **tr)
+    diagnostics_golden()
     print("golden vectors written to", OUT)
 
 
@@ -333,6 +343,66 @@ def _trace_cases(cp, c):
     out["solve_rf"] = np.asarray(rf)
     out["solve_depth"] = 2 * HALF_Z
     return out
+
+
+def diagnostics_golden():
+    """Ray-transfer-matrix diagnostics (src/processing/diagnostics.py): the
+    reference's own solve methods, histograms and module-level optics on
+    seeded Jones vectors (x, theta, y, phi), metres and radians."""
+    sym = types.ModuleType("sympy")
+    sym.Matrix = lambda *a, **k: np.asarray(*a)
+    sys.modules.setdefault("sympy", sym)
+    import processing.diagnostics as dg      # noqa: E402
+
+    rng = np.random.RandomState(4321)
+    N = 1500
+    rf = np.stack([rng.normal(0, 2e-3, N), rng.normal(0, 5e-3, N), rng.normal(0, 1.5e-3, N),
+                   rng.normal(0, 4e-3, N)]).astype(np.float32)
+    rf[:, 7] = np.nan
+    rf[0, 11] = np.nan
+    rf[3, 19] = np.nan
+    weights = rng.uniform(0.5, 1.0, N).astype(np.float32)
+    out = {"rf": rf, "weights": weights}
+
+    def run(name, cls, solve, init_kw, hist_kw, solve_kw=None, use_weights=True):
+        d = cls(rf.copy(), weights=weights.copy() if use_weights else None, **init_kw)
+        if solve is not None:
+            getattr(d, solve)(**(solve_kw or {}))
+        d.histogram(**hist_kw)
+        out[f"{name}_H"] = np.asarray(d.H, dtype=np.float64)
+        out[f"{name}_xedges"] = np.asarray(d.xedges)
+        out[f"{name}_yedges"] = np.asarray(d.yedges)
+        out[f"{name}_rf"] = np.asarray(d.rf, dtype=np.float64)
+
+    run("shadow_single", dg.Shadowgraphy, "single_lens_solve", dict(L=400, R=25, Lx=18, Ly=13.5),
+        dict(bin_scale=16))
+    run("shadow_two", dg.Shadowgraphy, "two_lens_solve", dict(focal_plane=1.0, L=400, R=25, Lx=18, Ly=13.5),
+        dict(bin_scale=8), use_weights=False)
+    run("shadow_custom", dg.Shadowgraphy, "single_lens_custom_solve",
+        dict(L=400, R=25, Lx=18, Ly=13.5, prefilter_input=True, ccd_shape_m=(10e-3, 8e-3)),
+        dict(bin_scale=12), solve_kw=dict(f=150, obj_dist=300, img_dist=600))
+    run("schlieren_df", dg.Schlieren, "DF_solve", dict(L=400, R=25, Lx=18, Ly=13.5), dict(bin_scale=16),
+        solve_kw=dict(R=1.0))
+    run("schlieren_lf", dg.Schlieren, "LF_solve", dict(L=400, R=25, Lx=18, Ly=13.5), dict(bin_scale=16),
+        solve_kw=dict(R=1.0))
+    run("refract", dg.Refractometry, "incoherent_solve", dict(L=400, R=25, Lx=18, Ly=13.5), dict(bin_scale=16))
+    run("refract_custom", dg.Refractometry, "incoherent_custom_solve", dict(L=400, R=25, Lx=18, Ly=13.5),
+        dict(bin_scale=16), solve_kw=dict(f1=150, f3=250, img_f1_dist=500, img_dist=350))
+    run("plain", dg.Shadowgraphy, None, dict(L=400, R=25, Lx=18, Ly=13.5), dict(bin_scale=16, plain_plot=True))
+    # module-level optics on a mm copy of the first 400 rays
+    r = dg.m_to_mm(rf[:, :400].astype(np.float64))
+    out["op_in"] = r
+    out["op_travel"] = dg.travel(r, 123.0)
+    out["op_lens"] = dg.lens(r, 80.0, -120.0)
+    out["op_circ_ap"] = dg.circular_aperture(r.copy(), 2.5)
+    out["op_circ_stop"] = dg.circular_stop(r.copy(), 1.5)
+    out["op_rect_ap"] = dg.rect_aperture(r.copy(), 2.0, 1.0)
+    out["op_annular_mask"] = dg.annular_stop(r.copy(), 1.0, 2.5)
+    out["op_knife_x_pos"] = dg.knife_edge(r.copy(), 0.5, "x", 1)
+    out["op_knife_y_neg"] = dg.knife_edge(r.copy(), -0.25, "y", -1)
+    out["op_lens_cutoff"] = dg.lens_cutoff(r.copy(), L=400, R=3)
+    np.savez_compressed(os.path.join(OUT, "diagnostics.npz"), **out)
+    print("diagnostics golden vectors written to", OUT)
 
 
 if __name__ == "__main__":
