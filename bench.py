@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=2000)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-diagnostics", action="store_true")
     return ap.parse_args()
 
 
@@ -243,6 +244,36 @@ def run_serving(args):
 
 
 # ---------------------------------------------------------------------------
+# diagnostics: the single-lens shadowgraphy chain and the transmission-
+# weighted 3448 x 2574 histogram of every traced ray, one K6 launch
+# ---------------------------------------------------------------------------
+def run_diagnostics(outs):
+    import torch
+    from sloth_b200.processing import diagnostics as dg
+    jv, amp = outs["jones"][-1], outs["amp"][-1]
+    n = int(jv.shape[1])
+    L = 400.0
+    ops = [(dg.TRAVEL, 3 * L / 4, 0, 0), (dg.CIRCULAR_APERTURE, 25.0, 0, 0), (dg.LENS, L / 2, L / 2, 0),
+           (dg.TRAVEL, 3 * L / 2, 0, 0)]
+    H = torch.zeros((2574, 3448), dtype=torch.float64, device=jv.device)
+    stream = torch.cuda.current_stream()
+    times = []
+    for it in range(8):
+        H.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dg.run_optics(jv, ops, weights=amp, pos_scale=1e3, hist=(3448, 2574, (-9.0, 9.0), (-6.75, 6.75)), out_hist=H)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if it >= 3:
+            times.append(e0.elapsed_time(e1))
+    ms = float(np.median(times))
+    return {"workload": f"Shadowgraphy.single_lens_solve + histogram (3448 x 2574, transmission weights) of the "
+                        f"{n:.0e} traced rays", "ms": ms, "rays_per_s": n / (ms / 1e3),
+            "binned_weight": float(H.sum()), "launches": 1}
+
+
+# ---------------------------------------------------------------------------
 # adjoint: d loss / d ne for a 256^2 detector image of 1e6 rays through a
 # 128^3 FP32 Kolmogorov grid (400 RK4 steps, checkpoints every 20, 2-pixel
 # splat); loss = ||I - I_target||^2 with I_target from another seeded field
@@ -319,21 +350,16 @@ def run_sloth(args):
     from sloth_b200.core import physics
     from sloth_b200.core.propagator import solve
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from sloth_b200 import replicas
+    world, rank, local = replicas.rank_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    dist = replicas.init(world, dev, "nccl")
 
     n, nrays = args.n, int(args.rays)
     h = L / (n - 1)
     omega = physics.omega_of(LWL)
-    seed = args.seed + 1000 * rank
+    seed = replicas.rank_seed(args.seed, rank)
     ne, rays = make_workload(n, nrays, seed, dev)
     grid = runtime.pack_grid(ne, (-L / 2,) * 3, (h, h, h), omega, precision="f32")
     sched = runtime.schedule_times([math.sqrt(8.0) * L], (h, h, h))
@@ -346,8 +372,7 @@ def run_sloth(args):
                              want_status=True, want_steps=False, outputs=outs, events=ev)
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        replicas.barrier(dist)
 
     for _ in range(args.warmup):
         step()
@@ -374,22 +399,14 @@ def run_sloth(args):
     kernel_ms = [a.elapsed_time(b) for a, b in kev]
     total_ms = evs[0][0].elapsed_time(evs[-1][1])
     ray_steps = int(outs["total_steps"][0])
-    if dist is not None:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t[0])
-        s = torch.tensor([ray_steps], device=dev, dtype=torch.float64)
-        dist.all_reduce(s)
-        all_ray_steps = float(s[0])
-    else:
-        all_ray_steps = float(ray_steps)
+    total_ms, all_ray_steps = replicas.job_totals(dist, total_ms, ray_steps, dev)
     value = all_ray_steps * args.steps / (total_ms / 1e3)
     f32_out = {k: v.clone() for k, v in outs.items()}
 
     # ---- all-FP64 port of the same kernel on the same workload -------------
     fp64 = None
     acc = None
-    if not args.no_fp64:
+    if not args.no_fp64 and world == 1:
         g64 = runtime.pack_grid(ne, (-L / 2,) * 3, (h, h, h), omega, precision="f64")
         r64 = rays.double()
         o64 = {}
@@ -458,6 +475,7 @@ def run_sloth(args):
             res = solve(rays_host, dom, L, lwl=LWL, verbose=False, detector_plane=L / 2, return_extras=True)
         torch.cuda.synchronize()
         reps = max(2, min(args.steps, 3))
+        barrier()
         t0 = time.perf_counter()
         for _ in range(reps):
             res = solve(rays_host, dom, L, lwl=LWL, verbose=False, detector_plane=L / 2, return_extras=True)
@@ -466,18 +484,26 @@ def run_sloth(args):
         rf, amp, _, ex = res
         d2h = rf.nbytes + amp.nbytes + ex["phase"].nbytes + ex["status"].nbytes + ex["steps"].nbytes
         h2d = ne_host.numel() * ne_host.element_size() + rays_host.numel() * rays_host.element_size()
-        e2e = {"value": ex["total_steps"] / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "ms_per_step": dt * 1e3,
+        # solve() returns host arrays, so each call ends synchronised; the
+        # per-rank time is host-measured and the job's is the max over ranks
+        dt_ms, steps_all = replicas.job_totals(dist, dt * 1e3, float(ex["total_steps"]), dev)
+        e2e = {"value": steps_all / (dt_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": dt_ms,
                "path": "sloth_b200.core.propagator.solve (pinned host ne and rays, numpy outputs)"}
+
+    # ---- diagnostics: shadowgraphy of the traced rays on a KAF-8300 ---------
+    diag = None
+    if not args.no_diagnostics and world == 1:
+        diag = run_diagnostics(f32_out)
 
     # ---- serving: the mixed request stream (p50/p99 latency) ----------------
     serve = None
-    if not args.no_serving:
+    if not args.no_serving and world == 1:
         serve = run_serving(args)
 
     # ---- adjoint: gradient of a detector-image loss -------------------------
     adj = None
-    if not args.no_adjoint:
+    if not args.no_adjoint and world == 1:
         adj = run_adjoint(args)
 
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
@@ -518,13 +544,12 @@ def run_sloth(args):
             "fp32_vs_fp64": acc,
             "serving": serve,
             "adjoint": adj,
+            "diagnostics": diag,
         }
         if fp64:
             line["fp64_port"]["speedup_of_fp32"] = value / world / fp64["value"]
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(dist)
 
 
 def main():
