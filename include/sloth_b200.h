@@ -362,6 +362,36 @@ int sloth_optics_f64(const double* rays, int64_t n, const double* weights, const
                      int32_t n_optics, const SlothDetectorParams* d, double* hist, double* rays_out,
                      uint8_t* kept, void* stream);
 
+/* ---- K7: probing beam on the device --------------------------------------
+ * The rays of the reference's Beam (src/core/beam.py:57-346), (6, n)
+ * row-major as Beam.s0: start plane probing_axis = ne_extent, speed c,
+ * polar angle divergence * N(0,1) from the probing axis, azimuth pi * U, and
+ * positions per beam_type (circular: radius size[0] * sqrt(U); square:
+ * size[0] * (2U - 1) on both axes; rectangular: size[0], size[1]; linear:
+ * size[0] * (2U - 1) on axis 0, velocity in the axis-0 / axis-2 plane).
+ * The random numbers are not numpy's RandomState stream: draw k of ray id is
+ * a hash of (seed, id, k). The rays [first_id, first_id + n) of one seed
+ * are the same whichever calls generate them. */
+#define SLOTH_BEAM_CIRCULAR     0
+#define SLOTH_BEAM_SQUARE       1
+#define SLOTH_BEAM_RECTANGULAR  2   /* also rect_trackers */
+#define SLOTH_BEAM_LINEAR       3
+
+typedef struct SlothBeamParams {
+    int32_t  beam_type;      /* SLOTH_BEAM_*                                       */
+    int32_t  probing_axis;   /* 0, 1, 2                                            */
+    double   size[2];        /* beam_size (m); size[1] for rectangular only        */
+    double   divergence;     /* rad                                                */
+    double   ne_extent;      /* start plane coordinate along probing_axis (m)      */
+    uint64_t seed;
+    uint64_t first_id;       /* id of the first ray generated by this call         */
+    int32_t  reserved;       /* must be 0                                          */
+    int32_t  reserved2;
+} SlothBeamParams;
+
+int sloth_beam_f32(const SlothBeamParams* p, int64_t n, float* s0, void* stream);
+int sloth_beam_f64(const SlothBeamParams* p, int64_t n, double* s0, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

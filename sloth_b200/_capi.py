@@ -100,6 +100,15 @@ class SlothDetectorParams(Structure):
 SLOTH_MAX_OPTICS = 32
 
 
+class SlothBeamParams(Structure):
+    _fields_ = [("beam_type", c_int32), ("probing_axis", c_int32), ("size", c_double * 2), ("divergence", c_double),
+                ("ne_extent", c_double), ("seed", ctypes.c_uint64), ("first_id", ctypes.c_uint64),
+                ("reserved", c_int32), ("reserved2", c_int32)]
+
+
+SLOTH_BEAM_CIRCULAR, SLOTH_BEAM_SQUARE, SLOTH_BEAM_RECTANGULAR, SLOTH_BEAM_LINEAR = 0, 1, 2, 3
+
+
 class SlothImageParams(Structure):
     _fields_ = [("dtau", c_double), ("n_steps", c_int32), ("ckpt_every", c_int32), ("probing_axis", c_int32),
                 ("n_px", c_int32 * 2), ("reserved", c_int32), ("plane", c_double), ("window", c_double * 4),
@@ -151,6 +160,8 @@ _SIGNATURES = {
                                  POINTER(SlothDetectorParams), c_void_p, c_void_p, c_void_p, c_void_p]),
     "sloth_optics_f64": (c_int, [c_void_p, c_int64, c_void_p, POINTER(SlothOptic), c_int32,
                                  POINTER(SlothDetectorParams), c_void_p, c_void_p, c_void_p, c_void_p]),
+    "sloth_beam_f32": (c_int, [POINTER(SlothBeamParams), c_int64, c_void_p, c_void_p]),
+    "sloth_beam_f64": (c_int, [POINTER(SlothBeamParams), c_int64, c_void_p, c_void_p]),
 }
 
 EXPORTED_SYMBOLS = tuple(_SIGNATURES)

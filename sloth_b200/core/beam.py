@@ -15,8 +15,18 @@ Differences, each a defect of the reference:
   raises NotImplementedError.
 * unknown beam types print a message and then fail on `del t` (:335-338);
   here they raise ValueError with that message.
+
+Keyword-only extra: ``device`` (e.g. 'cuda') generates the rays on the GPU
+(sloth_beam_f32) into a CUDA tensor ``s0``, for beams too large to draw on
+the host. Those rays follow the same distributions and placement, but their
+random numbers come from a counter-based hash of (seed, ray index), not from
+numpy's RandomState, so a seeded device beam is reproducible but is not the
+reference's seeded beam.
 """
 from __future__ import annotations
+
+import ctypes
+import secrets
 
 import numpy as np
 from scipy.constants import c
@@ -26,7 +36,7 @@ _VALID_TYPES = (int, float, np.integer, np.floating)
 
 class Beam:
     def __init__(self, Np, beam_size, divergence, ne_extent, *, probing_direction='z', beam_type='circular',
-                 seeded=False):
+                 seeded=False, device=None):
         self.Np = np.int64(Np)
         self.beam_size = beam_size
         self.divergence = divergence
@@ -34,7 +44,46 @@ class Beam:
         self.probing_direction = probing_direction
         self.beam_type = beam_type
         self.seed = 42 if seeded else None
-        Beam.init_beam(self, -self.ne_extent, self.seed)
+        if device is not None:
+            self._init_beam_device(-self.ne_extent, device)
+        else:
+            Beam.init_beam(self, -self.ne_extent, self.seed)
+
+    def _init_beam_device(self, ne_extent, device):
+        import torch
+        from .. import _capi as capi
+        from .. import runtime
+        bt = self.beam_type
+        kinds = {'circular': capi.SLOTH_BEAM_CIRCULAR, 'square': capi.SLOTH_BEAM_SQUARE,
+                 'rectangular': capi.SLOTH_BEAM_RECTANGULAR, 'rect_trackers': capi.SLOTH_BEAM_RECTANGULAR,
+                 'linear': capi.SLOTH_BEAM_LINEAR}
+        if bt == 'even':
+            raise NotImplementedError("beam_type 'even' produces no rays in the reference (src/core/beam.py:255-272)")
+        if bt not in kinds:
+            raise ValueError("\nself.beam_type unrecognised! Accepted args: circular, square, rectangular, linear, "
+                             "even, rect_trackers.")
+        if bt in ('rectangular', 'rect_trackers'):
+            assert len(self.beam_size) == 2, ("\nERROR: Must pass a list of length 2 to initialise a rectangular beam,"
+                                              + str(len(self.beam_size)) + "item was passed.")
+            size = (float(self.beam_size[0]), float(self.beam_size[1]))
+        else:
+            assert isinstance(self.beam_size, _VALID_TYPES), \
+                "\nReceived beam_size of shape" + str(np.shape(self.beam_size)) + "expected a float."
+            size = (float(self.beam_size), 0.0)
+        dev = runtime.require_device(device)
+        p = capi.SlothBeamParams()
+        p.beam_type = kinds[bt]
+        p.probing_axis = ['x', 'y', 'z'].index(self.probing_direction)
+        p.size[0], p.size[1] = size
+        p.divergence = float(self.divergence)
+        p.ne_extent = float(ne_extent)
+        p.seed = self.seed if self.seed is not None else secrets.randbits(64)
+        p.first_id = 0
+        n = int(self.Np)
+        s0 = torch.empty((6, n), dtype=torch.float32, device=dev)
+        capi.check(capi.load().sloth_beam_f32(ctypes.byref(p), n, capi.ptr(s0),
+                                              torch.cuda.current_stream(dev).cuda_stream), "sloth_beam_f32")
+        self.s0 = s0
 
     def init_beam(self, ne_extent, seed):
         rng = np.random.RandomState(seed)

@@ -183,3 +183,55 @@ def test_error_codes_from_device_entry_points():
     with pytest.raises(_capi.SlothError) as e:
         runtime.pack_grid(torch.from_numpy(ne), origin, spacing, omega, out=bad)
     assert e.value.code == _capi.SLOTH_ERR_MISALIGNED
+
+
+def _noncubic_case(axis, nrays=2000, seed=3):
+    """A (72, 40, 56)-point grid over 6 x 4 x 5 mm (three spacings), a smooth
+    density with structure on every axis, rays entering through the low face
+    of `axis` with 1 mrad of jitter."""
+    n = (72, 40, 56)
+    ext = (6e-3, 4e-3, 5e-3)
+    h = tuple(e / (k - 1) for e, k in zip(ext, n))
+    origin = tuple(-e / 2 for e in ext)
+    c = [origin[a] + h[a] * np.arange(n[a]) for a in range(3)]
+    X, Y, Z = np.meshgrid(*c, indexing="ij")
+    ne = (1e25 * (1 + 0.2 * np.sin(2 * np.pi * X / 1.3e-3) * np.cos(2 * np.pi * Y / 0.9e-3)
+                  + 0.15 * np.sin(2 * np.pi * Z / 1.7e-3 + 0.4))).astype(np.float32)
+    rng = np.random.RandomState(seed)
+    rays = np.zeros((6, nrays), np.float32)
+    for a in range(3):
+        if a == axis:
+            rays[a] = origin[a]
+        else:
+            rays[a] = rng.normal(0, ext[a] / 6, nrays)
+    d = np.zeros((3, nrays))
+    d[axis] = 1.0
+    for a in range(3):
+        if a != axis:
+            d[a] = rng.normal(0, 1e-3, nrays)
+    d /= np.linalg.norm(d, axis=0)
+    rays[3:] = (d * C).astype(np.float32)
+    sched = runtime.schedule_times(np.linspace(0.0, ext[axis], 3), h)
+    return ne, rays, origin, h, 2 * np.pi * C / 532e-9, sched, ext
+
+
+@pytest.mark.parametrize("axis", [0, 1])
+def test_noncubic_anisotropic_grid(axis):
+    ne, rays, origin, h, omega, sched, ext = _noncubic_case(axis)
+    kw = dict(axis=axis, project=True, plane=ext[axis] / 2, inv_brems=True, Te=20.0, Z=1.0)
+    o = run_oracle(ne, rays, origin, h, omega, sched, **kw)
+    k64 = run_kernel(ne, rays, origin, h, omega, sched, precision="f64", **kw)
+    Lmax = max(ext)
+    assert position_error(k64["state"], o["state"], Lmax) < 1e-10
+    assert direction_error(k64["state"], o["state"]) < 1e-10
+    np.testing.assert_allclose(k64["phase"], o["phase"], rtol=0, atol=1e-10 * np.abs(o["phase"]).max())
+    np.testing.assert_allclose(k64["amp"], o["amp"], rtol=0, atol=1e-12)
+    k32 = run_kernel(ne, rays, origin, h, omega, sched, precision="f32", **kw)
+    assert position_error(k32["state"], o["state"], Lmax) < 1e-6
+    assert direction_error(k32["state"], o["state"]) < 1e-6
+    t = [a for a in range(3) if a != axis]
+    far = (np.abs(o["state"][-1][t[0]]) <= ext[t[0]] / 2) & (np.abs(o["state"][-1][t[1]]) <= ext[t[1]] / 2)
+    assert far.mean() > 0.9
+    ph = np.abs(o["phase"]).max()
+    assert np.abs(k32["phase"] - o["phase"])[:, far].max() <= 1e-6 * ph
+    assert np.abs(k32["amp"].astype(np.float64) - o["amp"])[:, far].max() < 1e-6
