@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define SLOTH_ABI_VERSION 1
+#define SLOTH_ABI_VERSION 2
 
 /* ---- return codes ------------------------------------------------------ */
 #define SLOTH_OK                        0
@@ -82,6 +82,13 @@ typedef struct SlothTraceParams {
     double  q_max;            /* upper bound of ne/nc over the grid, or 0 if unknown;
                                  a bound selects faster exact paths (sub-critical
                                  kappa; series n - 1 when (omega_pe/omega)^2 <= 0.05) */
+    double  q_min;            /* lower bound of ne/nc over the grid (0 for a density
+                                 known to be >= 0). With q_max it bounds the ray's
+                                 acceleration; when that bound keeps every stage point
+                                 of an interior step inside the grid, those steps skip
+                                 the per-stage grid test (same results, fewer
+                                 instructions). A value above the true minimum is an
+                                 error of the caller. */
 } SlothTraceParams;
 
 #define SLOTH_MAX_SAVES 4096

@@ -61,7 +61,7 @@ class SlothTraceParams(Structure):
                 ("first_save", c_int32), ("save_every", c_int32), ("n_saves", c_int32),
                 ("probing_axis", c_int32), ("project_to_plane", c_int32), ("inv_brems", c_int32),
                 ("plane", c_double), ("kappa_q2", c_double), ("coulomb_log_w", c_double),
-                ("ope_ratio2", c_double), ("q_max", c_double)]
+                ("ope_ratio2", c_double), ("q_max", c_double), ("q_min", c_double)]
 
 
 class SlothTraceOutputs(Structure):

@@ -6,7 +6,7 @@
 
 namespace sloth {
 
-template <class P, int IB, bool SMALLX>
+template <class P, int IB, bool SMALLX, bool FAST>
 __global__ void __launch_bounds__(kThreads, SLOTH_TRACE_MIN_BLOCKS)
 trace_kernel(const __grid_constant__ TraceArgs a) {
     __shared__ unsigned s_key[kTile];
@@ -27,30 +27,35 @@ trace_kernel(const __grid_constant__ TraceArgs a) {
         if (tile >= a.n_tiles) break;
         const long long start = (long long)tile * kTile;
         const int cnt = (int)min((long long)kTile, a.n - start);
-        trace_tile<P, IB, SMALLX>(a, start, cnt, s_key, s_id, &s_head, cc, my_steps);
+        trace_tile<P, IB, SMALLX, FAST>(a, start, cnt, s_key, s_id, &s_head, cc, my_steps);
     }
     // one atomic per CTA for the ray-step total
     block_add(my_steps, &s_steps, a.total_steps);
 }
 
-template <class P, int IB, bool SMALLX>
-static int launch_trace(const TraceArgs& ta, int sms, cudaStream_t s) {
+template <class P, int IB, bool SMALLX, bool FAST>
+static int launch_trace_k(const TraceArgs& ta, int sms, cudaStream_t s) {
     static int cached[64] = {0};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_status(e);
     int per_sm = (dev >= 0 && dev < 64) ? cached[dev] : 0;
     if (per_sm <= 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel<P, IB, SMALLX>, kThreads, 0) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel<P, IB, SMALLX, FAST>, kThreads, 0) !=
                 cudaSuccess || per_sm < 1)
             per_sm = 1;
         if (dev >= 0 && dev < 64) cached[dev] = per_sm;
     }
     long long blocks = (long long)sms * per_sm;
     if (blocks > ta.n_tiles) blocks = ta.n_tiles;
-    trace_kernel<P, IB, SMALLX><<<(int)blocks, kThreads, 0, s>>>(ta);
+    trace_kernel<P, IB, SMALLX, FAST><<<(int)blocks, kThreads, 0, s>>>(ta);
     note_launch();
     return cuda_status(cudaGetLastError());
+}
+
+template <class P, int IB, bool SMALLX>
+static int launch_trace(const TraceArgs& ta, int sms, cudaStream_t s, bool fast) {
+    return fast ? launch_trace_k<P, IB, SMALLX, true>(ta, sms, s) : launch_trace_k<P, IB, SMALLX, false>(ta, sms, s);
 }
 
 template <class P>
@@ -103,18 +108,19 @@ static int trace_impl(const SlothGridDesc* g, const void* grid, const SlothTrace
     int ib;
     bool smallx;
     trace_mode(p, &ib, &smallx);
+    const bool fast = interior_bound_ok(g, p);
 
     if (out->trace_event_begin) {
         e = cudaEventRecord((cudaEvent_t)out->trace_event_begin, s);
         if (e != cudaSuccess) return cuda_status(e);
     }
     if (ib == IB_OFF)
-        rc = smallx ? launch_trace<P, IB_OFF, true>(ta, sms, s) : launch_trace<P, IB_OFF, false>(ta, sms, s);
+        rc = smallx ? launch_trace<P, IB_OFF, true>(ta, sms, s, fast) : launch_trace<P, IB_OFF, false>(ta, sms, s, fast);
     else if (ib == IB_SUBCRITICAL)
-        rc = smallx ? launch_trace<P, IB_SUBCRITICAL, true>(ta, sms, s)
-                    : launch_trace<P, IB_SUBCRITICAL, false>(ta, sms, s);
+        rc = smallx ? launch_trace<P, IB_SUBCRITICAL, true>(ta, sms, s, fast)
+                    : launch_trace<P, IB_SUBCRITICAL, false>(ta, sms, s, fast);
     else
-        rc = launch_trace<P, IB_GENERAL, false>(ta, sms, s);
+        rc = launch_trace<P, IB_GENERAL, false>(ta, sms, s, fast);
     if (rc) return rc;
     if (out->trace_event_end) {
         e = cudaEventRecord((cudaEvent_t)out->trace_event_end, s);

@@ -54,6 +54,21 @@ constexpr double kSmallX = 0.05;         // bound on (omega_pe/omega)^2 for the 
 // Inverse-bremsstrahlung modes of the tracer.
 enum { IB_OFF = 0, IB_SUBCRITICAL = 1, IB_GENERAL = 2 };
 
+// How a step samples its stage points: PLAIN tests each point against the
+// grid (fill 0 outside); CLAMP moves it into the grid first (steps at a
+// face); INTERIOR skips the test, for steps whose stage points are known to
+// lie inside (see interior_bound_ok). Every mode clamps the cell index into
+// the grid, so no mode can read outside the grid.
+enum { SAMPLE_PLAIN = 0, SAMPLE_CLAMP = 1, SAMPLE_INTERIOR = 2 };
+
+// Largest |acceleration| (cells per step^2) for which an interior step
+// (ray inside, prediction p + w at least kFaceMargin inside on every axis)
+// has every stage point inside: the stages sit at p + w/2 + A1/4 and
+// p + w + A2/2, at least kFaceMargin/2 and kFaceMargin from the faces before
+// the A terms, so |A| <= 4 * (kFaceMargin/2) = 0.04 suffices; 0.03 keeps
+// headroom for rounding.
+constexpr double kInteriorAccel = 0.03;
+
 // ---------------------------------------------------------------------------
 // Kernel arguments.
 // ---------------------------------------------------------------------------
@@ -184,7 +199,7 @@ __device__ __forceinline__ typename P::R corner_kappa(const TraceArgs& a, typena
 // rounded sum; the weights from (hi - i) + lo, which resolves the position
 // inside the cell to FP32 relative precision rather than FP32 precision of
 // the absolute position. CLAMP moves the point into the grid first.
-template <class P, int IB, bool CLAMP, class Cache>
+template <class P, int IB, int MODE, class Cache>
 __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R (&hi)[3],
                                          const typename P::R (&lo)[3], Sample<P>& out, Cache& cc) {
     using R = typename P::R;
@@ -196,7 +211,7 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
         h[x] = hi[x];
         l[x] = lo[x];
         p[x] = h[x] + l[x];
-        if constexpr (CLAMP) {
+        if constexpr (MODE == SAMPLE_CLAMP) {
             const R pc = fmin(fmax(p[x], R(0)), lim_of<R>(g, x));
             if (pc != p[x]) {
                 h[x] = pc;
@@ -205,15 +220,22 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
             }
         }
     }
-    const bool in = (p[0] >= R(0)) & (p[0] <= lim_of<R>(g, 0)) & (p[1] >= R(0)) &
-                    (p[1] <= lim_of<R>(g, 1)) & (p[2] >= R(0)) & (p[2] <= lim_of<R>(g, 2));
-    if (!in) {
-        out.q = out.g0 = out.g1 = out.g2 = out.k = R(0);
-        return;
+    int ix, iy, iz;
+    if constexpr (MODE != SAMPLE_INTERIOR) {
+        const bool in = (p[0] >= R(0)) & (p[0] <= lim_of<R>(g, 0)) & (p[1] >= R(0)) &
+                        (p[1] <= lim_of<R>(g, 1)) & (p[2] >= R(0)) & (p[2] <= lim_of<R>(g, 2));
+        if (!in) {
+            out.q = out.g0 = out.g1 = out.g2 = out.k = R(0);
+            return;
+        }
+        ix = min((int)p[0], g.n[0] - 2);
+        iy = min((int)p[1], g.n[1] - 2);
+        iz = min((int)p[2], g.n[2] - 2);
+    } else {
+        ix = min(max((int)p[0], 0), g.n[0] - 2);
+        iy = min(max((int)p[1], 0), g.n[1] - 2);
+        iz = min(max((int)p[2], 0), g.n[2] - 2);
     }
-    const int ix = min((int)p[0], g.n[0] - 2);
-    const int iy = min((int)p[1], g.n[1] - 2);
-    const int iz = min((int)p[2], g.n[2] - 2);
     const R fx = (h[0] - (R)ix) + l[0], fy = (h[1] - (R)iy) + l[1], fz = (h[2] - (R)iz) + l[2];
     const unsigned b = (unsigned)ix * g.sx + (unsigned)iy * g.sy + (unsigned)iz;
     if constexpr (P::cell_poly) {
@@ -312,7 +334,7 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
 //   with w2 = w + phi*A1/2, w3 = w + phi*A2/2.
 // The phase integrand is n - 1 with n = sqrt(1 - (omega_pe/omega)^2) from the
 // interpolated density (src/legacy/full_solver.py:271-274, :341-347).
-template <class P, int IB, bool SMALLX, bool CLAMP, class Cache>
+template <class P, int IB, bool SMALLX, int MODE, class Cache>
 __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
     using R = typename P::R;
     const R two = R(2);
@@ -328,7 +350,7 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
     }
     Sample<P> s;
     // stage 1 at p
-    sample_c<P, IB, CLAMP>(a, ph, pl, s, cc);
+    sample_c<P, IB, MODE>(a, ph, pl, s, cc);
     R g = nm1<P, SMALLX>(ope2 * s.q);
     R kq = s.k;
     sA[0] = S0 * s.g0; sA[1] = S1 * s.g1; sA[2] = S2 * s.g2;
@@ -338,7 +360,7 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
         sW[x] = sA[x];
         st[x] = pl[x] + hphi * we[x];
     }
-    sample_c<P, IB, CLAMP>(a, ph, st, s, cc);
+    sample_c<P, IB, MODE>(a, ph, st, s, cc);
 #pragma unroll
     for (int x = 0; x < 3; ++x) st[x] = pl[x] + hphi * (we[x] + hphi * sA[x]);   // p + phi*w2/2
     {
@@ -353,7 +375,7 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
     g += two * nm1<P, SMALLX>(ope2 * s.q);
     kq += two * s.k;
     // stage 3 at p + phi*w2/2
-    sample_c<P, IB, CLAMP>(a, ph, st, s, cc);
+    sample_c<P, IB, MODE>(a, ph, st, s, cc);
     {
         const R A[3] = {S0 * s.g0, S1 * s.g1, S2 * s.g2};
 #pragma unroll
@@ -366,7 +388,7 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
     g += two * nm1<P, SMALLX>(ope2 * s.q);
     kq += two * s.k;
     // stage 4 at p + phi*w3
-    sample_c<P, IB, CLAMP>(a, ph, st, s, cc);
+    sample_c<P, IB, MODE>(a, ph, st, s, cc);
     sW[0] += S0 * s.g0; sW[1] += S1 * s.g1; sW[2] += S2 * s.g2;
     g += nm1<P, SMALLX>(ope2 * s.q);
     kq += s.k;
@@ -582,7 +604,7 @@ __device__ __forceinline__ void tile_sort(unsigned* key, unsigned* id) {
 // trace them one thread per ray, refilling finished lanes from the tile
 // (warp ballot + shared-memory atomic). *s_head must be 0 on entry and the
 // block must be synchronised. Shared by the single-trace and serving kernels.
-template <class P, int IB, bool SMALLX, class Cache>
+template <class P, int IB, bool SMALLX, bool FAST, class Cache>
 __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, int cnt, unsigned* s_key,
                                            unsigned* s_id, int* s_head, Cache& cc,
                                            unsigned long long& my_steps) {
@@ -624,10 +646,12 @@ __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, 
         if (active) {
             typename P::R phi;
             const int kind = step_kind<P>(a, r, phi);
-            if (kind == 0 || kind == 3) {
-                rk4_step<P, IB, SMALLX, false>(a, r, cc, typename P::R(1));
+            if (FAST && kind == 0) {
+                rk4_step<P, IB, SMALLX, SAMPLE_INTERIOR>(a, r, cc, typename P::R(1));
+            } else if (kind == 0 || kind == 3) {
+                rk4_step<P, IB, SMALLX, SAMPLE_PLAIN>(a, r, cc, typename P::R(1));
             } else {
-                rk4_step<P, IB, SMALLX, true>(a, r, cc, phi);
+                rk4_step<P, IB, SMALLX, SAMPLE_CLAMP>(a, r, cc, phi);
                 if (kind == 2) {
                     r.exited = true;
                     r.lag = 1.0 - (double)phi;
@@ -861,6 +885,20 @@ inline int check_trace_params(const SlothGridDesc* g, const SlothTraceParams* p,
     if (p->project_to_plane && !std::isfinite(p->plane)) return SLOTH_ERR_INVALID_ARGUMENT;
     if (!std::isfinite(p->q_max)) return SLOTH_ERR_INVALID_ARGUMENT;
     return SLOTH_OK;
+}
+
+// True when interior steps may skip the per-stage grid test: the
+// acceleration |S_k * dq/du_k| is at most max_k |S_k| * (q_max - min(q_min, 0))
+// (a difference of q over at most one cell), and that is within
+// kInteriorAccel. Needs q_max > 0 (known) and q_min <= q_max.
+inline bool interior_bound_ok(const SlothGridDesc* g, const SlothTraceParams* p) {
+    if (!(p->q_max > 0.0) || !std::isfinite(p->q_min) || !(p->q_min <= p->q_max)) return false;
+    double smax = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        const double r = p->dtau / g->spacing[k];
+        smax = fmax(smax, 0.5 * r * r);
+    }
+    return smax * (p->q_max - fmin(p->q_min, 0.0)) <= kInteriorAccel;
 }
 
 // Tracer mode of a trace: inverse-bremsstrahlung path and phase form.

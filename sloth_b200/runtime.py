@@ -62,6 +62,7 @@ class DeviceGrid:
     origin: tuple
     spacing: tuple
     q_max: float = 0.0         # max of the q channel (ne/nc) over the grid; 0 = unknown
+    q_min: float = float("inf")  # a lower bound of min(q, 0) over the grid; inf = unknown
 
     @property
     def nc(self) -> float:
@@ -106,9 +107,13 @@ def pack_grid(ne, origin, spacing, omega, *, precision="f32", device=None, strea
     scale = 1.0 / physics.critical_density(omega) if ne_scale is None else float(ne_scale)
     capi.check(fn(desc, capi.ptr(ne), int(ne.dtype == torch.float64), scale, capi.ptr(out), _stream_ptr(stream)),
                "sloth_grid_pack")
-    q_max = float(ne.max()) * scale if ne.numel() else 0.0
+    if ne.numel():
+        lo, hi = torch.aminmax(ne)
+        q_max, q_min = float(hi) * scale, float(lo) * scale
+    else:
+        q_max, q_min = 0.0, 0.0
     return DeviceGrid(out, desc, precision, float(omega), n, tuple(map(float, origin)), tuple(map(float, spacing)),
-                      q_max=max(q_max, 0.0) * (1.0 + 1e-6))
+                      q_max=max(q_max, 0.0) * (1.0 + 1e-6), q_min=min(q_min, 0.0) * (1.0 + 1e-6))
 
 
 def sample(grid: DeviceGrid, points, *, stream=None) -> torch.Tensor:
@@ -231,6 +236,7 @@ def trace(grid: DeviceGrid, rays: torch.Tensor, sched: Schedule, *, axis=2, proj
     else:
         p.kappa_q2, p.coulomb_log_w, p.ope_ratio2 = 0.0, 2.0, physics.ope_ratio2(grid.omega)
     p.q_max = float(grid.q_max)
+    p.q_min = float(grid.q_min)
     out = capi.SlothTraceOutputs()
     out.jones = capi.ptr(jones)
     out.state = capi.ptr(state)

@@ -235,3 +235,22 @@ def test_noncubic_anisotropic_grid(axis):
     ph = np.abs(o["phase"]).max()
     assert np.abs(k32["phase"] - o["phase"])[:, far].max() <= 1e-6 * ph
     assert np.abs(k32["amp"].astype(np.float64) - o["amp"])[:, far].max() < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_interior_fast_path_is_bitwise_identical(precision):
+    """With a known density range the tracer skips the per-stage grid test on
+    interior steps; the results must not change at all."""
+    import dataclasses
+    ne, rays, origin, spacing, omega = case("kolmogorov", 48, 3000, seed=21, jitter=2e-3)
+    sched = _sched(48, 3, False)
+    g = runtime.pack_grid(torch.from_numpy(ne), origin, spacing, omega, precision=precision)
+    assert g.q_min <= 0.0 < g.q_max
+    dt = torch.float32 if precision == "f32" else torch.float64
+    r = torch.from_numpy(rays).to("cuda", dt)
+    kw = dict(project=True, plane=L / 2, inv_brems=True, Te=20.0, Z=1.0, want_state=True)
+    fast = runtime.trace(g, r, sched, **kw)
+    slow = runtime.trace(dataclasses.replace(g, q_min=float("inf")), r, sched, **kw)
+    torch.cuda.synchronize()
+    for key in ("jones", "state", "phase", "amp", "status", "steps", "total_steps"):
+        assert torch.equal(fast[key], slow[key]), key
