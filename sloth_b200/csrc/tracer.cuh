@@ -44,6 +44,9 @@
 #ifndef SLOTH_TRACE_MIN_BLOCKS
 #define SLOTH_TRACE_MIN_BLOCKS 2
 #endif
+#ifndef SLOTH_PAIRED_F32
+#define SLOTH_PAIRED_F32 1
+#endif
 
 namespace sloth {
 
@@ -161,6 +164,46 @@ __device__ __forceinline__ R poly_eval(const R (&t)[8], R fx, R fy, R fz) {
     return ((t[0] + fx * t[1]) + fy * cy) + fz * cz;
 }
 
+// FP32 cell cache on paired instructions. The packed voxel is a float4
+// (q, dq/du, dq/dv, dq/dw), so (q, dq/du) and (dq/dv, dq/dw) arrive in
+// register pairs; each pair of trilinear polynomials is built and evaluated
+// with sm_100's two-wide FP32 instructions (__fadd2/__ffma2: one instruction
+// for two channels, each component rounded exactly as the scalar operation).
+// The inverse-bremsstrahlung channel (NK = 5) stays scalar.
+template <int NK>
+struct CellPolyF2 {
+    unsigned base;
+    float2 t[2][8];
+    float k[NK == 5 ? 8 : 1];
+};
+
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);          // a - b, one rounding
+}
+
+__device__ __forceinline__ void poly_coeffs2(float2 (&t)[8], float2 v0, float2 v1, float2 v2, float2 v3, float2 v4,
+                                             float2 v5, float2 v6, float2 v7) {
+    const float2 bz = sub2(v1, v0), by = sub2(v2, v0), bx = sub2(v4, v0);
+    const float2 dyz = sub2(v3, v2), dxz = sub2(v5, v4), dxy = sub2(v6, v4);
+    t[0] = v0;
+    t[1] = bx;
+    t[2] = by;
+    t[3] = bz;
+    t[4] = sub2(dxy, by);
+    t[5] = sub2(dxz, bz);
+    t[6] = sub2(dyz, bz);
+    t[7] = sub2(sub2(sub2(v7, v6), dxz), sub2(dyz, bz));
+}
+
+__device__ __forceinline__ float2 poly_eval2(const float2 (&t)[8], float2 fx, float2 fy, float2 fz) {
+    const float2 cz = __ffma2_rn(fy, __ffma2_rn(fx, t[7], t[6]), __ffma2_rn(fx, t[5], t[3]));
+    const float2 cy = __ffma2_rn(fx, t[4], t[2]);
+    return __ffma2_rn(fz, cz, __ffma2_rn(fy, cy, __ffma2_rn(fx, t[1], t[0])));
+}
+
+template <class C> struct IsPairedCache : std::false_type {};
+template <int NK> struct IsPairedCache<CellPolyF2<NK>> : std::true_type {};
+
 // n - 1 for n = sqrt(1 - x), x = (omega_pe/omega)^2. SMALLX (FP32 only, used
 // when x <= kSmallX over the whole grid) takes the binomial series
 // -(x/2 + x^2/8 + x^3/16 + 5x^4/128 + 7x^5/256), whose first omitted term is
@@ -238,7 +281,46 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
     }
     const R fx = (h[0] - (R)ix) + l[0], fy = (h[1] - (R)iy) + l[1], fz = (h[2] - (R)iz) + l[2];
     const unsigned b = (unsigned)ix * g.sx + (unsigned)iy * g.sy + (unsigned)iz;
-    if constexpr (P::cell_poly) {
+    if constexpr (IsPairedCache<Cache>::value) {
+        if (b != cc.base) {
+            cc.base = b;
+            const float4* gp = reinterpret_cast<const float4*>(a.grid);
+            const float4 v0 = __ldg(gp + b), v1 = __ldg(gp + b + 1u);
+            const float4 v2 = __ldg(gp + b + g.sy), v3 = __ldg(gp + b + g.sy + 1u);
+            const float4 v4 = __ldg(gp + b + g.sx), v5 = __ldg(gp + b + g.sx + 1u);
+            const float4 v6 = __ldg(gp + b + g.sx + g.sy), v7 = __ldg(gp + b + g.sx + g.sy + 1u);
+#define SLOTH_LO(v) make_float2(v.x, v.y)
+#define SLOTH_HI(v) make_float2(v.z, v.w)
+            poly_coeffs2(cc.t[0], SLOTH_LO(v0), SLOTH_LO(v1), SLOTH_LO(v2), SLOTH_LO(v3), SLOTH_LO(v4), SLOTH_LO(v5),
+                         SLOTH_LO(v6), SLOTH_LO(v7));
+            poly_coeffs2(cc.t[1], SLOTH_HI(v0), SLOTH_HI(v1), SLOTH_HI(v2), SLOTH_HI(v3), SLOTH_HI(v4), SLOTH_HI(v5),
+                         SLOTH_HI(v6), SLOTH_HI(v7));
+#undef SLOTH_LO
+#undef SLOTH_HI
+            if constexpr (IB == IB_SUBCRITICAL) {
+                poly_coeffs<float>(cc.k, v0.x * v0.x, v1.x * v1.x, v2.x * v2.x, v3.x * v3.x, v4.x * v4.x,
+                                   v5.x * v5.x, v6.x * v6.x, v7.x * v7.x);
+            } else if constexpr (IB == IB_GENERAL) {
+                poly_coeffs<float>(cc.k, corner_kappa<P>(a, v0.x), corner_kappa<P>(a, v1.x), corner_kappa<P>(a, v2.x),
+                                   corner_kappa<P>(a, v3.x), corner_kappa<P>(a, v4.x), corner_kappa<P>(a, v5.x),
+                                   corner_kappa<P>(a, v6.x), corner_kappa<P>(a, v7.x));
+            }
+        }
+        const float2 fx2 = make_float2(fx, fx), fy2 = make_float2(fy, fy), fz2 = make_float2(fz, fz);
+        const float2 r0 = poly_eval2(cc.t[0], fx2, fy2, fz2);
+        const float2 r1 = poly_eval2(cc.t[1], fx2, fy2, fz2);
+        out.q = r0.x;
+        out.g0 = r0.y;
+        out.g1 = r1.x;
+        out.g2 = r1.y;
+        if constexpr (IB == IB_SUBCRITICAL) {
+            out.k = poly_eval<float>(cc.k, fx, fy, fz) * (float)a.cl_lo;
+        } else if constexpr (IB == IB_GENERAL) {
+            out.k = poly_eval<float>(cc.k, fx, fy, fz);
+        } else {
+            out.k = 0.0f;
+        }
+    } else if constexpr (P::cell_poly) {
         if (b != cc.base) {
             cc.base = b;
             const V v0 = P::load(a.grid, b), v1 = P::load(a.grid, b + 1u);
@@ -666,7 +748,11 @@ __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, 
 
 // Register cache of the last cell: polynomial coefficients or corners.
 template <class P, int IB>
-using CellCacheFor = typename std::conditional<P::cell_poly, CellPoly<P, (IB != IB_OFF) ? 5 : 4>, CellCache<P>>::type;
+using CellCacheFor = typename std::conditional<
+    P::cell_poly,
+    typename std::conditional<std::is_same<typename P::R, float>::value && SLOTH_PAIRED_F32,
+                              CellPolyF2<(IB != IB_OFF) ? 5 : 4>, CellPoly<P, (IB != IB_OFF) ? 5 : 4>>::type,
+    CellCache<P>>::type;
 
 // Sum of `v` over the block, added to *dst by one thread.
 __device__ __forceinline__ void block_add(unsigned long long v, unsigned long long* s_acc,
