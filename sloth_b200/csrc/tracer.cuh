@@ -88,6 +88,9 @@ struct TraceArgs {
     double w_of_v[3];          // w = v * w_of_v   (cells per step per m/s)
     double v_of_w[3];          // v = w * v_of_w
     double S[3];               // -(dtau/h)^2 / 2
+    float Sf[3];               // the same, rounded to FP32 once here (the FP32 tracer reads these
+                               // instead of converting the doubles inside its loop)
+    float ope2f, cl_lof, cl_wf;
     double phase_scale;        // (omega/c) * dtau / 6
     double tau_scale;          // kappa_q2 * dtau / 6
     double cl_w, cl_lo;        // Coulomb log below nc, and max(2, cl_w)
@@ -104,6 +107,20 @@ struct TraceArgs {
     int32_t* steps;
     unsigned long long* total_steps;
 };
+
+// Scalar parameters in the tracer's precision (FP32 copies made on the host).
+template <class R> __device__ __forceinline__ R arg_S(const TraceArgs& a, int k);
+template <> __device__ __forceinline__ float arg_S<float>(const TraceArgs& a, int k) { return a.Sf[k]; }
+template <> __device__ __forceinline__ double arg_S<double>(const TraceArgs& a, int k) { return a.S[k]; }
+template <class R> __device__ __forceinline__ R arg_ope2(const TraceArgs& a) {
+    if constexpr (sizeof(R) == 4) return a.ope2f; else return a.ope2;
+}
+template <class R> __device__ __forceinline__ R arg_cl_lo(const TraceArgs& a) {
+    if constexpr (sizeof(R) == 4) return a.cl_lof; else return a.cl_lo;
+}
+template <class R> __device__ __forceinline__ R arg_cl_w(const TraceArgs& a) {
+    if constexpr (sizeof(R) == 4) return a.cl_wf; else return a.cl_w;
+}
 
 __device__ __forceinline__ double sel3(const double (&v)[3], int i) {
     return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]);
@@ -223,8 +240,8 @@ __device__ __forceinline__ typename P::R nm1(typename P::R x) {
 template <class P>
 __device__ __forceinline__ typename P::R corner_kappa(const TraceArgs& a, typename P::R q) {
     using R = typename P::R;
-    const R x = q * (R)a.ope2;
-    const R cl = (x > R(1)) ? fmax(R(2), (R)a.cl_w - R(0.5) * P::log_(x)) : (R)a.cl_lo;
+    const R x = q * arg_ope2<R>(a);
+    const R cl = (x > R(1)) ? fmax(R(2), arg_cl_w<R>(a) - R(0.5) * P::log_(x)) : arg_cl_lo<R>(a);
     return q * q * cl;
 }
 
@@ -314,7 +331,7 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
         out.g1 = r1.x;
         out.g2 = r1.y;
         if constexpr (IB == IB_SUBCRITICAL) {
-            out.k = poly_eval<float>(cc.k, fx, fy, fz) * (float)a.cl_lo;
+            out.k = poly_eval<float>(cc.k, fx, fy, fz) * a.cl_lof;
         } else if constexpr (IB == IB_GENERAL) {
             out.k = poly_eval<float>(cc.k, fx, fy, fz);
         } else {
@@ -345,7 +362,7 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
         out.g1 = poly_eval<R>(cc.t[2], fx, fy, fz);
         out.g2 = poly_eval<R>(cc.t[3], fx, fy, fz);
         if constexpr (IB == IB_SUBCRITICAL) {
-            out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz) * (R)a.cl_lo;
+            out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz) * arg_cl_lo<R>(a);
         } else if constexpr (IB == IB_GENERAL) {
             out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz);
         } else {
@@ -396,7 +413,7 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
             R k = R(0);
     #pragma unroll
             for (int i = 0; i < 8; ++i) k += w[i] * (c[i].x * c[i].x);
-            out.k = k * (R)a.cl_lo;
+            out.k = k * arg_cl_lo<R>(a);
         } else if constexpr (IB == IB_GENERAL) {
             R k = R(0);
     #pragma unroll
@@ -421,8 +438,8 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
     using R = typename P::R;
     const R two = R(2);
     const R hphi = R(0.5) * phi, phi6 = phi * R(1.0 / 6.0), phi2_6 = phi * phi6;
-    const R S0 = (R)a.S[0], S1 = (R)a.S[1], S2 = (R)a.S[2];
-    const R ope2 = (R)a.ope2;
+    const R S0 = arg_S<R>(a, 0), S1 = arg_S<R>(a, 1), S2 = arg_S<R>(a, 2);
+    const R ope2 = arg_ope2<R>(a);
     R ph[3], pl[3], we[3], sA[3], sW[3], w3[3], st[3];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
@@ -930,12 +947,16 @@ inline void fill_trace_args(TraceArgs& ta, const SlothGridDesc* g, const void* g
         ta.w_of_v[k] = (p->dtau / h) / kC;
         ta.v_of_w[k] = kC * h / p->dtau;
         ta.S[k] = -0.5 * (p->dtau / h) * (p->dtau / h);
+        ta.Sf[k] = (float)ta.S[k];
     }
     ta.phase_scale = (p->omega / kC) * p->dtau / 6.0;
     ta.tau_scale = p->kappa_q2 * p->dtau / 6.0;
     ta.cl_w = p->coulomb_log_w;
     ta.cl_lo = p->coulomb_log_w > 2.0 ? p->coulomb_log_w : 2.0;
     ta.ope2 = p->ope_ratio2;
+    ta.ope2f = (float)ta.ope2;
+    ta.cl_lof = (float)ta.cl_lo;
+    ta.cl_wf = (float)ta.cl_w;
     ta.plane = p->plane;
     ta.first_save = p->first_save;
     ta.save_every = p->n_saves > 1 ? p->save_every : 1;
