@@ -628,26 +628,30 @@ __device__ __forceinline__ void finish_ray(const TraceArgs& a, const Ray<P>& r, 
 // while the ray still needs steps. `check_gone` is false after a plain step
 // taken from inside the grid with its prediction more than kFaceMargin inside
 // (the ray cannot have left); the outside test is skipped then.
+//
+// Most steps need nothing here, which the first test decides with integer
+// compares. The rest goes through one loop with a single emit call site: a
+// save due now is taken at the ray's time (lag), and a ray that has left
+// the grid for good takes all its remaining saves by straight-line drift.
+// (Two emit call sites with the same arguments let the compiler hoist their
+// common part, the state's FP64 conversions and the Jones angles, into
+// every step.)
 template <class P>
 __device__ __forceinline__ bool settle(const TraceArgs& a, Ray<P>& r, unsigned long long& my_steps,
                                       bool check_gone = true) {
-    while (r.save_j < a.n_saves && r.next_save == r.step) {
-        emit<P>(a, r, r.lag);
+    const bool leaving = r.exited || (check_gone && ray_gone<P>(a, r));
+    if (r.next_save != r.step && !leaving) return true;
+    while (r.save_j < a.n_saves) {
+        const bool due = r.next_save == r.step;
+        if (!due && !leaving) break;
+        const double drift = due ? r.lag : (double)(r.next_save - r.step) + r.lag;
+        emit<P>(a, r, drift);
         ++r.save_j;
         r.next_save += a.save_every;
     }
     if (r.save_j >= a.n_saves) {
         finish_ray<P>(a, r, (!r.exited && ray_in_grid<P>(a, r)) ? SLOTH_RAY_INSIDE_AT_END : SLOTH_RAY_EXITED,
                       my_steps);
-        return false;
-    }
-    if (r.exited || (check_gone && ray_gone<P>(a, r))) {
-        while (r.save_j < a.n_saves) {
-            emit<P>(a, r, (double)(r.next_save - r.step) + r.lag);
-            ++r.save_j;
-            r.next_save += a.save_every;
-        }
-        finish_ray<P>(a, r, SLOTH_RAY_EXITED, my_steps);
         return false;
     }
     return true;
