@@ -58,12 +58,10 @@ def _scalar(v, name):
     raise NotImplementedError(f"spatially varying {name} is not supported by the B200 tracers; pass a scalar")
 
 
-def _check_overcritical(ne, omega, stacklevel=3):
+def _check_overcritical(ne, omega, stacklevel=3, ne_max=None):
     ncr = physics.critical_density(omega)
-    if isinstance(ne, torch.Tensor):
-        ne_max = float(ne.max())
-    else:
-        ne_max = float(np.max(ne))
+    if ne_max is None:
+        ne_max = float(ne.max()) if isinstance(ne, torch.Tensor) else float(np.max(ne))
     if ne_max >= ncr:
         warnings.warn(
             f"precompute_gradients: {ne_max:.3g} m⁻³ cells at or above critical density ncr = {ncr:.3g} m⁻³ "
@@ -84,8 +82,10 @@ def device_grid(domain, omega, *, precision="f32", device=None, stream=None):
         ne = np.asarray(ne)
     if tuple(ne.shape) != tuple(n):
         raise ValueError(f"ne has shape {tuple(ne.shape)} but the coordinates give {tuple(n)}")
-    _check_overcritical(ne, omega, stacklevel=4)
-    return runtime.pack_grid(ne, origin, spacing, omega, precision=precision, device=device, stream=stream)
+    g = runtime.pack_grid(ne, origin, spacing, omega, precision=precision, device=device, stream=stream)
+    # the warning uses the maximum the pack's device reduction already found
+    _check_overcritical(ne, omega, stacklevel=4, ne_max=g.ne_max)
+    return g
 
 
 def precompute_gradients(ne, x, y, z, omega, *, device=None):
@@ -219,28 +219,38 @@ def solve(beam, ScalarDomain, probing_depth, *, parallelise=True, jitted=True, s
     duration = np.float64(time.time() - start)
     if verbose:
         print("\nCompleted ray trace in", np.round(duration, 3), "seconds.")
+    # results to host memory: every copy queued, then one synchronisation
+    want = {}
+    if return_raw_results:
+        want["state"] = out["state"]
+        if inv_brems:
+            want["amp"] = out["amp"]
+    else:
+        want["jones"] = out["jones"][-1] if S <= 2 else out["jones"]
+        if S <= 2 and inv_brems:
+            want["amp"] = out["amp"][-1]
+    if return_extras:
+        for k in ("phase", "status", "steps", "total_steps"):
+            want[k] = out[k]
+    host = dict(zip(want, runtime.to_host(*want.values())))
     extras = None
     if return_extras:
-        extras = {"phase": out["phase"].cpu().numpy(), "status": out["status"].cpu().numpy(),
-                  "steps": out["steps"].cpu().numpy(), "total_steps": int(out["total_steps"].item()),
-                  "precision": precision}
+        extras = {"phase": host["phase"], "status": host["status"], "steps": host["steps"],
+                  "total_steps": int(host["total_steps"][0]), "precision": precision}
 
     def ret(*v):
         return (*v, extras) if return_extras else v
 
     if return_raw_results:
-        st = out["state"].cpu().numpy()                      # (S, 6, N)
-        ys = np.transpose(st, (2, 0, 1))
+        ys = np.transpose(host["state"], (2, 0, 1))          # (N, S, 6)
         if inv_brems:
-            tau = -np.log(out["amp"].cpu().numpy().astype(np.float64))   # (S, N)
+            tau = -np.log(host["amp"].astype(np.float64))    # (S, N)
             ys = np.concatenate([ys, tau.T[:, :, None]], axis=2)
         ts = np.broadcast_to(np.linspace(0.0, 1.0, S)[None, :], (ys.shape[0], S))
         return ret(np.asarray([RawSolution(ys, ts)], dtype=object), None, duration)
-    jones = out["jones"].cpu().numpy()
     if S <= 2:
-        amp = out["amp"][-1].cpu().numpy() if inv_brems else None
-        return ret(jones[-1], amp, duration)
-    return ret(jones, None, duration)
+        return ret(host["jones"], host.get("amp"), duration)
+    return ret(host["jones"], None, duration)
 
 
 # ---------------------------------------------------------------------------
@@ -289,16 +299,18 @@ def trace_and_save_depths(beam, ScalarDomain, step, depth_max, output_path, *, l
     sched = runtime.schedule_times(depth_saves, grid.spacing)
     r = _rays_tensor(s0, precision, dev)
     out = runtime.trace(grid, r, sched, axis=axis, inv_brems=inv_brems, Te=Te, Z=Z, stream=stream)
-    jones = out["jones"].cpu().numpy()
+    keys = ["jones"] + (["amp"] if inv_brems else []) + (["phase", "status", "steps"] if return_extras else [])
+    host = dict(zip(keys, runtime.to_host(*(out[k] for k in keys))))
+    jones = host["jones"]
     jvec = [np.asarray(jones[j])[comp, :] for j in range(n_saves)]
     result = {'depth_saves': depth_saves, 'jvec': jvec, 'jones_components': comp}
     if inv_brems:
-        amp = out["amp"].cpu().numpy()
+        amp = host["amp"]
         result['amplitude'] = [np.asarray(amp[j]) for j in range(n_saves)]
     if return_extras:
-        result['phase'] = [p for p in out["phase"].cpu().numpy()]
-        result['status'] = out["status"].cpu().numpy()
-        result['steps'] = out["steps"].cpu().numpy()
+        result['phase'] = [p for p in host["phase"]]
+        result['status'] = host["status"]
+        result['steps'] = host["steps"]
     if output_path is not None:
         with open(output_path, 'wb') as fh:
             pickle.dump(result, fh)

@@ -63,6 +63,7 @@ class DeviceGrid:
     spacing: tuple
     q_max: float = 0.0         # max of the q channel (ne/nc) over the grid; 0 = unknown
     q_min: float = float("inf")  # a lower bound of min(q, 0) over the grid; inf = unknown
+    ne_max: float = float("nan")  # largest ne (m^-3) packed, from the device reduction
 
     @property
     def nc(self) -> float:
@@ -109,11 +110,26 @@ def pack_grid(ne, origin, spacing, omega, *, precision="f32", device=None, strea
                "sloth_grid_pack")
     if ne.numel():
         lo, hi = torch.aminmax(ne)
-        q_max, q_min = float(hi) * scale, float(lo) * scale
+        ne_max = float(hi)
+        q_max, q_min = ne_max * scale, float(lo) * scale
     else:
-        q_max, q_min = 0.0, 0.0
+        ne_max, q_max, q_min = 0.0, 0.0, 0.0
     return DeviceGrid(out, desc, precision, float(omega), n, tuple(map(float, origin)), tuple(map(float, spacing)),
-                      q_max=max(q_max, 0.0) * (1.0 + 1e-6), q_min=min(q_min, 0.0) * (1.0 + 1e-6))
+                      q_max=max(q_max, 0.0) * (1.0 + 1e-6), q_min=min(q_min, 0.0) * (1.0 + 1e-6), ne_max=ne_max)
+
+
+def to_host(*tensors):
+    """Device tensors -> numpy arrays through pinned host buffers (PyTorch's
+    caching host allocator reuses them across calls): asynchronous copies on
+    the current stream, one synchronisation."""
+    outs = []
+    for t in tensors:
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t, non_blocking=True)
+        outs.append(h)
+    if tensors:
+        torch.cuda.current_stream(tensors[0].device).synchronize()
+    return [h.numpy() for h in outs]
 
 
 def sample(grid: DeviceGrid, points, *, stream=None) -> torch.Tensor:
