@@ -106,8 +106,10 @@ class RayServer:
         if grid_key not in self._qmax:
             if ne is None:
                 raise ValueError("ne is required for a grid key seen for the first time")
-            self._qmax[grid_key] = float(ne.max()) / physics.critical_density(omega) * (1 + 1e-6)
-        p.q_max = self._qmax[grid_key]
+            lo, hi = torch.aminmax(ne)
+            nc = physics.critical_density(omega)
+            self._qmax[grid_key] = (max(float(hi) / nc, 0.0) * (1 + 1e-6), min(float(lo) / nc, 0.0) * (1 + 1e-6))
+        p.q_max, p.q_min = self._qmax[grid_key]
         if rays.dtype != torch.float32 or not rays.is_contiguous():
             raise ValueError("rays must be a contiguous float32 (6, N) tensor")
         on_host = rays.device.type == "cpu"
