@@ -42,6 +42,9 @@
 namespace sloth {
 
 constexpr int kAdjThreads = 256;
+// The FP32 backward fits in 128 registers (two 256-thread CTAs per SM) with a
+// few bytes of spill; the FP64 one would spill kilobytes, so it keeps one.
+template <class P> constexpr int adj_bwd_min_blocks() { return sizeof(typename P::R) == 4 ? 2 : 1; }
 constexpr int kMaxCkptEvery = 32;
 constexpr int kMaxTaps = 65;          // 2 * 4 * sigma + 1 pixels at sigma <= 8
 
@@ -519,7 +522,7 @@ __global__ void __launch_bounds__(kAdjThreads) image_forward_kernel(const __grid
 }
 
 template <class P>
-__global__ void __launch_bounds__(kAdjThreads) image_backward_kernel(const __grid_constant__ ImageArgs a) {
+__global__ void __launch_bounds__(kAdjThreads, adj_bwd_min_blocks<P>()) image_backward_kernel(const __grid_constant__ ImageArgs a) {
     using R = typename P::R;
     const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= a.n) return;
