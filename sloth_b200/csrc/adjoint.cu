@@ -203,7 +203,8 @@ __device__ __forceinline__ void accel(const ImageArgs& a, const typename P::R (&
 //   p' = p + w + (A1 + A2 + A3)/6,  w' = w + (A1 + 2A2 + 2A3 + A4)/6,
 //   stages at p, p + w/2, p + w/2 + A1/4, p + w + A2/2.
 template <class P>
-__device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, GradCell<P>& cc) {
+__device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, GradCell<P>& cc,
+                                           typename P::R* A1out = nullptr, typename P::R* A2out = nullptr) {
     using R = typename P::R;
     R ph[3], pl[3], we[3], st[3], A1[3], A2[3], A3[3], A4[3];
 #pragma unroll
@@ -222,6 +223,13 @@ __device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, Gra
 #pragma unroll
     for (int x = 0; x < 3; ++x) st[x] = pl[x] + (we[x] + R(0.5) * A2[x]);
     accel<P>(a, ph, st, A4, cc);
+    if (A1out) {
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            A1out[x] = A1[x];
+            A2out[x] = A2[x];
+        }
+    }
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         const R sA = (A1[x] + A2[x]) + A3[x];
@@ -316,21 +324,19 @@ __device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const typename
 // Reverse of model_step from the step's input state r: (lp, lw) = adjoint of
 // the output (p', w') on entry, of the input (p, w) on return.
 template <class P>
-__device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const MState<P>& r, typename P::R (&lp)[3],
-                                                   typename P::R (&lw)[3], GradCell<P>& cc, CornerAcc<P>& acc) {
+__device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const MState<P>& r,
+                                                   const typename P::R (&A1)[3], const typename P::R (&A2)[3],
+                                                   typename P::R (&lp)[3], typename P::R (&lw)[3], GradCell<P>& cc,
+                                                   CornerAcc<P>& acc) {
     using R = typename P::R;
-    R ph[3], pl[3], we[3], st[3], A1[3], A2[3];
+    R ph[3], pl[3], we[3], st[3];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         ph[x] = r.p[x].hi();
         pl[x] = r.p[x].lo();
         we[x] = r.w[x].val();
     }
-    // stage accelerations that place the later stages
-    accel<P>(a, ph, pl, A1, cc);
-#pragma unroll
-    for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * we[x];
-    accel<P>(a, ph, st, A2, cc);
+    // A1, A2 (which place stages 3 and 4) come from the segment's recompute
     R a1[3], a2[3], a3[3], a4[3], pb[3], wb[3], q[3];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
@@ -556,16 +562,22 @@ __global__ void __launch_bounds__(kAdjThreads, adj_bwd_min_blocks<P>()) image_ba
     cc.base = kNone;
     CornerAcc<P> acc;
     acc.base = kNone;
+    // a segment's step inputs and their first two stage accelerations
     MState<P> seg[kMaxCkptEvery];
+    R segA[kMaxCkptEvery][6];
     for (int s = (T + a.ckpt_every - 1) / a.ckpt_every - 1; s >= 0; --s) {
         load_state<P>(a, s, slot, r);
         const int j0 = s * a.ckpt_every;
         const int m = min(a.ckpt_every, T - j0);
         for (int j = 0; j < m; ++j) {
             seg[j] = r;
-            if (j + 1 < m) model_step<P>(a, r, cc);
+            model_step<P>(a, r, cc, &segA[j][0], &segA[j][3]);
         }
-        for (int j = m - 1; j >= 0; --j) model_step_adjoint<P>(a, seg[j], lp, lw, cc, acc);
+        for (int j = m - 1; j >= 0; --j) {
+            const R A1[3] = {segA[j][0], segA[j][1], segA[j][2]};
+            const R A2[3] = {segA[j][3], segA[j][4], segA[j][5]};
+            model_step_adjoint<P>(a, seg[j], A1, A2, lp, lw, cc, acc);
+        }
     }
     flush<P>(a, acc);
 }
