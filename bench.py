@@ -234,6 +234,8 @@ def run_serving(args):
            "seconds": live["seconds"],
            "saturated_ray_steps_per_s": sat["ray_steps_per_s"], "saturated_seconds": sat["seconds"],
            "iterations": live["stats"]["iterations"], "grid_packs": live["stats"]["grid_packs"],
+           "gpu_busy_frac": live["stats"]["gpu_busy_ms"] / max(live["stats"]["gpu_span_ms"], 1e-9),
+           "saturated_gpu_busy_frac": sat["stats"]["gpu_busy_ms"] / max(sat["stats"]["gpu_span_ms"], 1e-9),
            "budget_bytes": live["stats"]["budget_bytes"],
            "stream": "2000 requests, Poisson 200/s, grids {64,128,192,256,384}^3 sinusoid|Kolmogorov, "
                      "lognormal rays median 2e5 sigma 1 in [1e4, 4e6], 120 GB budget; latency = arrival to "

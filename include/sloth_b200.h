@@ -196,6 +196,8 @@ typedef struct SlothServerStats {
     long long grids_resident, grid_packs, grid_evictions;
     long long jobs_submitted, jobs_admitted, jobs_done, jobs_failed;
     long long iterations, tiles, kernel_launches;
+    double    gpu_busy_ms;   /* time some iteration was running on the GPU (union)  */
+    double    gpu_span_ms;   /* first iteration start to last finished iteration end */
 } SlothServerStats;
 
 #define SLOTH_JOB_PENDING  0

@@ -81,7 +81,7 @@ class SlothServerStats(Structure):
                 ("jobs_submitted", ctypes.c_longlong), ("jobs_admitted", ctypes.c_longlong),
                 ("jobs_done", ctypes.c_longlong), ("jobs_failed", ctypes.c_longlong),
                 ("iterations", ctypes.c_longlong), ("tiles", ctypes.c_longlong),
-                ("kernel_launches", ctypes.c_longlong)]
+                ("kernel_launches", ctypes.c_longlong), ("gpu_busy_ms", c_double), ("gpu_span_ms", c_double)]
 
 
 class SlothOptic(Structure):

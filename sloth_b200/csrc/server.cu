@@ -207,6 +207,7 @@ struct Job {
 struct IterSlot {
     cudaStream_t stream = nullptr;
     cudaGraphExec_t exec = nullptr;
+    cudaEvent_t start = nullptr;    // timing events around the iteration's graph
     cudaEvent_t done = nullptr;
     WorkHeader* h_buf = nullptr;    // pinned: header + items
     WorkHeader* d_buf = nullptr;    // device copy
@@ -231,6 +232,9 @@ struct ServerImpl {
     long long iter_next = 0;
     long long iter_done = -1;          // every iteration <= iter_done has finished
     std::set<long long> finished;      // finished iterations above iter_done
+    cudaEvent_t t0 = nullptr;          // time origin of the iteration intervals
+    std::map<long long, std::pair<double, double>> intervals;   // finished, not yet merged (ms from t0)
+    double busy_end = 0.0, first_start = -1.0;
     IterSlot it[2];
     cudaStream_t admit = nullptr;   // uploads, packing, pre-pass, table rows
     cudaStream_t copy = nullptr;    // result downloads
@@ -435,6 +439,10 @@ static void retire(ServerImpl* s) {
     for (IterSlot& is : s->it) {
         if (is.iter >= 0 && cudaEventQuery(is.done) == cudaSuccess) {
             s->finished.insert(is.iter);
+            float a = 0.f, b = 0.f;
+            if (cudaEventElapsedTime(&a, s->t0, is.start) == cudaSuccess &&
+                cudaEventElapsedTime(&b, s->t0, is.done) == cudaSuccess)
+                s->intervals[is.iter] = {a, b};
             is.iter = -1;
         }
     }
@@ -442,6 +450,21 @@ static void retire(ServerImpl* s) {
     while (!s->finished.empty() && *s->finished.begin() == s->iter_done + 1) {
         s->iter_done = *s->finished.begin();
         s->finished.erase(s->finished.begin());
+        // GPU-busy time: union of the iteration intervals, taken in iteration
+        // (= start) order
+        auto it = s->intervals.find(s->iter_done);
+        if (it != s->intervals.end()) {
+            const double a = it->second.first, b = it->second.second;
+            if (s->stats.gpu_span_ms == 0.0 && s->first_start < 0.0) s->first_start = a;
+            if (a >= s->busy_end) {
+                s->stats.gpu_busy_ms += b - a;
+            } else if (b > s->busy_end) {
+                s->stats.gpu_busy_ms += b - s->busy_end;
+            }
+            if (b > s->busy_end) s->busy_end = b;
+            s->stats.gpu_span_ms = s->busy_end - s->first_start;
+            s->intervals.erase(it);
+        }
     }
     cudaGetLastError();   // cudaErrorNotReady from the queries
     // jobs whose every tile ran in a finished iteration
@@ -507,6 +530,7 @@ static int launch_iteration(ServerImpl* s) {
     }
     cudaError_t e = cudaEventRecord(s->admit_ev, s->admit);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(is->stream, s->admit_ev, 0);
+    if (e == cudaSuccess) e = cudaEventRecord(is->start, is->stream);
     if (e == cudaSuccess) e = cudaGraphLaunch(is->exec, is->stream);
     if (e == cudaSuccess) e = cudaEventRecord(is->done, is->stream);
     if (e != cudaSuccess) return cuda_status(e);
@@ -554,7 +578,8 @@ int sloth_server_create(const SlothServerConfig* cfg, SlothServer** out) {
         (e = cudaMallocHost(&s->h_table, sizeof(sloth::TraceArgs) * cfg->max_jobs)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&s->admit, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&s->admit_ev, cudaEventDisableTiming)) != cudaSuccess)
+        (e = cudaEventCreateWithFlags(&s->admit_ev, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreate(&s->t0)) != cudaSuccess || (e = cudaEventRecord(s->t0, s->admit)) != cudaSuccess)
         return fail(sloth::cuda_status(e));
     for (int i = cfg->max_jobs - 1; i >= 0; --i) s->free_slots.push_back(i);
     int blocks[sloth::kModes] = {sloth::resident_blocks<sloth::IB_OFF, false>(s->sms),
@@ -565,7 +590,7 @@ int sloth_server_create(const SlothServerConfig* cfg, SlothServer** out) {
     const size_t wbytes = sizeof(sloth::WorkHeader) + sizeof(sloth::WorkItem) * (size_t)cfg->tiles_per_step;
     for (auto& is : s->it) {
         if ((e = cudaStreamCreateWithFlags(&is.stream, cudaStreamNonBlocking)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&is.done, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreate(&is.done)) != cudaSuccess || (e = cudaEventCreate(&is.start)) != cudaSuccess ||
             (e = cudaMallocHost(&is.h_buf, wbytes)) != cudaSuccess ||
             (e = cudaMalloc(&is.d_buf, wbytes)) != cudaSuccess)
             return fail(sloth::cuda_status(e));
@@ -589,11 +614,13 @@ int sloth_server_destroy(SlothServer* srv) {
     for (auto& is : s->it) {
         if (is.exec) cudaGraphExecDestroy(is.exec);
         if (is.done) cudaEventDestroy(is.done);
+        if (is.start) cudaEventDestroy(is.start);
         if (is.h_buf) cudaFreeHost(is.h_buf);
         if (is.d_buf) cudaFree(is.d_buf);
         if (is.stream) cudaStreamDestroy(is.stream);
     }
     if (s->admit_ev) cudaEventDestroy(s->admit_ev);
+    if (s->t0) cudaEventDestroy(s->t0);
     if (s->admit) cudaStreamDestroy(s->admit);
     if (s->copy) cudaStreamDestroy(s->copy);
     if (s->d_table) cudaFree(s->d_table);
