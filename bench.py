@@ -539,7 +539,13 @@ def run_sloth(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": f"{peak_kind} HBM copy bandwidth",
                          "kernel": "trace_kernel<PolF32>", "kernel_ms": kms,
-                         "bytes_per_ray_step": BYTES_PER_RAY_STEP},
+                         "bytes_per_ray_step": BYTES_PER_RAY_STEP,
+                         "dram_achieved": (traffic / (kms / 1e3) / 1e9) if traffic else None,
+                         "dram_frac": (traffic / (kms / 1e3) / 1e9 / peak) if traffic else None,
+                         "note": "achieved = logical gather bytes (4 RK4 stages x 8 corners x 16 B per ray-step); "
+                                 "the corners come from a register cell cache and L1, so physical DRAM traffic "
+                                 "(traffic, dram_frac, from ncu) is ~1.6 B per ray-step; the kernel is bound by "
+                                 "instruction issue (ncu summary in profiles/)"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),

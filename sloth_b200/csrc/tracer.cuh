@@ -292,9 +292,10 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
         iy = min((int)p[1], g.n[1] - 2);
         iz = min((int)p[2], g.n[2] - 2);
     } else {
-        ix = min(max((int)p[0], 0), g.n[0] - 2);
-        iy = min(max((int)p[1], 0), g.n[1] - 2);
-        iz = min(max((int)p[2], 0), g.n[2] - 2);
+        // one unsigned min clamps both ends (a negative index wraps to a large value)
+        ix = (int)min((unsigned)(int)p[0], (unsigned)(g.n[0] - 2));
+        iy = (int)min((unsigned)(int)p[1], (unsigned)(g.n[1] - 2));
+        iz = (int)min((unsigned)(int)p[2], (unsigned)(g.n[2] - 2));
     }
     const R fx = (h[0] - (R)ix) + l[0], fy = (h[1] - (R)iy) + l[1], fz = (h[2] - (R)iz) + l[2];
     const unsigned b = (unsigned)ix * g.sx + (unsigned)iy * g.sy + (unsigned)iz;
