@@ -235,6 +235,16 @@ __device__ __forceinline__ typename P::R nm1(typename P::R x) {
     }
 }
 
+// The FP32 series of nm1 for two arguments at once (sm_100 paired FP32).
+__device__ __forceinline__ float2 nm1_series2(float2 x) {
+    const float2 c = make_float2(0.02734375f, 0.02734375f);
+    float2 t = __ffma2_rn(x, c, make_float2(0.0390625f, 0.0390625f));
+    t = __ffma2_rn(x, t, make_float2(0.0625f, 0.0625f));
+    t = __ffma2_rn(x, t, make_float2(0.125f, 0.125f));
+    t = __ffma2_rn(x, t, make_float2(0.5f, 0.5f));
+    return __fmul2_rn(make_float2(-x.x, -x.y), t);
+}
+
 // Inverse-bremsstrahlung rate of one grid point per kappa_q2: q^2 * CL(q),
 // CL = max(2, cl_w - ln(max(omega_pe/omega, 1))) (src/core/propagator.py:155-162).
 template <class P>
@@ -450,8 +460,17 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
     }
     Sample<P> s;
     // stage 1 at p
+    // FP32 with the series form of n - 1 evaluates it for stages (1, 2) and
+    // (3, 4) as pairs
+    constexpr bool kPairPhase = SMALLX && sizeof(R) == 4;
     sample_c<P, IB, MODE>(a, ph, pl, s, cc);
-    R g = nm1<P, SMALLX>(ope2 * s.q);
+    R g, q1 = R(0), q3 = R(0);
+    if constexpr (kPairPhase) {
+        q1 = s.q;
+        g = R(0);
+    } else {
+        g = nm1<P, SMALLX>(ope2 * s.q);
+    }
     R kq = s.k;
     sA[0] = S0 * s.g0; sA[1] = S1 * s.g1; sA[2] = S2 * s.g2;
     // stage 2 at p + phi*w/2
@@ -472,7 +491,12 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
             sW[x] += two * A[x];
         }
     }
-    g += two * nm1<P, SMALLX>(ope2 * s.q);
+    if constexpr (kPairPhase) {
+        const float2 n12 = nm1_series2(__fmul2_rn(make_float2(ope2, ope2), make_float2(q1, s.q)));
+        g = n12.x + two * n12.y;
+    } else {
+        g += two * nm1<P, SMALLX>(ope2 * s.q);
+    }
     kq += two * s.k;
     // stage 3 at p + phi*w2/2
     sample_c<P, IB, MODE>(a, ph, st, s, cc);
@@ -485,12 +509,21 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
             st[x] = pl[x] + phi * w3[x];
         }
     }
-    g += two * nm1<P, SMALLX>(ope2 * s.q);
+    if constexpr (kPairPhase) {
+        q3 = s.q;
+    } else {
+        g += two * nm1<P, SMALLX>(ope2 * s.q);
+    }
     kq += two * s.k;
     // stage 4 at p + phi*w3
     sample_c<P, IB, MODE>(a, ph, st, s, cc);
     sW[0] += S0 * s.g0; sW[1] += S1 * s.g1; sW[2] += S2 * s.g2;
-    g += nm1<P, SMALLX>(ope2 * s.q);
+    if constexpr (kPairPhase) {
+        const float2 n34 = nm1_series2(__fmul2_rn(make_float2(ope2, ope2), make_float2(q3, s.q)));
+        g += two * n34.x + n34.y;
+    } else {
+        g += nm1<P, SMALLX>(ope2 * s.q);
+    }
     kq += s.k;
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
