@@ -47,6 +47,9 @@
 #ifndef SLOTH_PAIRED_F32
 #define SLOTH_PAIRED_F32 1
 #endif
+#ifndef SLOTH_PAIRED_STEP
+#define SLOTH_PAIRED_STEP 1
+#endif
 
 namespace sloth {
 
@@ -255,6 +258,35 @@ __device__ __forceinline__ typename P::R corner_kappa(const TraceArgs& a, typena
     return q * q * cl;
 }
 
+// Loads cell b into the paired cache: its polynomial coefficients, two
+// channels per instruction.
+template <class P, int IB, int NK>
+__device__ __forceinline__ void paired_fill(const TraceArgs& a, unsigned b, CellPolyF2<NK>& cc) {
+    const GridGeo& g = a.geo;
+    cc.base = b;
+    const float4* gp = reinterpret_cast<const float4*>(a.grid);
+    const float4 v0 = __ldg(gp + b), v1 = __ldg(gp + b + 1u);
+    const float4 v2 = __ldg(gp + b + g.sy), v3 = __ldg(gp + b + g.sy + 1u);
+    const float4 v4 = __ldg(gp + b + g.sx), v5 = __ldg(gp + b + g.sx + 1u);
+    const float4 v6 = __ldg(gp + b + g.sx + g.sy), v7 = __ldg(gp + b + g.sx + g.sy + 1u);
+#define SLOTH_LO(v) make_float2(v.x, v.y)
+#define SLOTH_HI(v) make_float2(v.z, v.w)
+    poly_coeffs2(cc.t[0], SLOTH_LO(v0), SLOTH_LO(v1), SLOTH_LO(v2), SLOTH_LO(v3), SLOTH_LO(v4), SLOTH_LO(v5),
+                 SLOTH_LO(v6), SLOTH_LO(v7));
+    poly_coeffs2(cc.t[1], SLOTH_HI(v0), SLOTH_HI(v1), SLOTH_HI(v2), SLOTH_HI(v3), SLOTH_HI(v4), SLOTH_HI(v5),
+                 SLOTH_HI(v6), SLOTH_HI(v7));
+#undef SLOTH_LO
+#undef SLOTH_HI
+    if constexpr (IB == IB_SUBCRITICAL) {
+        poly_coeffs<float>(cc.k, v0.x * v0.x, v1.x * v1.x, v2.x * v2.x, v3.x * v3.x, v4.x * v4.x, v5.x * v5.x,
+                           v6.x * v6.x, v7.x * v7.x);
+    } else if constexpr (IB == IB_GENERAL) {
+        poly_coeffs<float>(cc.k, corner_kappa<P>(a, v0.x), corner_kappa<P>(a, v1.x), corner_kappa<P>(a, v2.x),
+                           corner_kappa<P>(a, v3.x), corner_kappa<P>(a, v4.x), corner_kappa<P>(a, v5.x),
+                           corner_kappa<P>(a, v6.x), corner_kappa<P>(a, v7.x));
+    }
+}
+
 // Trilinear sample of the packed grid (rules of src/core/interpolator.py:79-104:
 // cell i = floor(p) clamped to [0, n-2], product weights, fill 0 outside)
 // returning q, the three gradient channels and, when IB, the interpolated
@@ -310,30 +342,7 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
     const R fx = (h[0] - (R)ix) + l[0], fy = (h[1] - (R)iy) + l[1], fz = (h[2] - (R)iz) + l[2];
     const unsigned b = (unsigned)ix * g.sx + (unsigned)iy * g.sy + (unsigned)iz;
     if constexpr (IsPairedCache<Cache>::value) {
-        if (b != cc.base) {
-            cc.base = b;
-            const float4* gp = reinterpret_cast<const float4*>(a.grid);
-            const float4 v0 = __ldg(gp + b), v1 = __ldg(gp + b + 1u);
-            const float4 v2 = __ldg(gp + b + g.sy), v3 = __ldg(gp + b + g.sy + 1u);
-            const float4 v4 = __ldg(gp + b + g.sx), v5 = __ldg(gp + b + g.sx + 1u);
-            const float4 v6 = __ldg(gp + b + g.sx + g.sy), v7 = __ldg(gp + b + g.sx + g.sy + 1u);
-#define SLOTH_LO(v) make_float2(v.x, v.y)
-#define SLOTH_HI(v) make_float2(v.z, v.w)
-            poly_coeffs2(cc.t[0], SLOTH_LO(v0), SLOTH_LO(v1), SLOTH_LO(v2), SLOTH_LO(v3), SLOTH_LO(v4), SLOTH_LO(v5),
-                         SLOTH_LO(v6), SLOTH_LO(v7));
-            poly_coeffs2(cc.t[1], SLOTH_HI(v0), SLOTH_HI(v1), SLOTH_HI(v2), SLOTH_HI(v3), SLOTH_HI(v4), SLOTH_HI(v5),
-                         SLOTH_HI(v6), SLOTH_HI(v7));
-#undef SLOTH_LO
-#undef SLOTH_HI
-            if constexpr (IB == IB_SUBCRITICAL) {
-                poly_coeffs<float>(cc.k, v0.x * v0.x, v1.x * v1.x, v2.x * v2.x, v3.x * v3.x, v4.x * v4.x,
-                                   v5.x * v5.x, v6.x * v6.x, v7.x * v7.x);
-            } else if constexpr (IB == IB_GENERAL) {
-                poly_coeffs<float>(cc.k, corner_kappa<P>(a, v0.x), corner_kappa<P>(a, v1.x), corner_kappa<P>(a, v2.x),
-                                   corner_kappa<P>(a, v3.x), corner_kappa<P>(a, v4.x), corner_kappa<P>(a, v5.x),
-                                   corner_kappa<P>(a, v6.x), corner_kappa<P>(a, v7.x));
-            }
-        }
+        if (b != cc.base) paired_fill<P, IB>(a, b, cc);
         const float2 fx2 = make_float2(fx, fx), fy2 = make_float2(fy, fy), fz2 = make_float2(fz, fz);
         const float2 r0 = poly_eval2(cc.t[0], fx2, fy2, fz2);
         const float2 r1 = poly_eval2(cc.t[1], fx2, fy2, fz2);
@@ -533,6 +542,176 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
     }
     r.ph += (double)(phi * g);
     if constexpr (IB != IB_OFF) r.tau.add(phi * kq);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 with the paired cell cache: the y and z components of every
+// per-axis quantity of the step travel as one register pair and use sm_100's
+// paired FP32 instructions (the cell polynomials already deliver dq/dv and
+// dq/dw as a pair); x stays scalar. Each component is rounded exactly as the
+// scalar step rounds it.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+
+// sample at (hx + lx, hyz + lyz)
+template <int IB, int MODE, int NK>
+__device__ __forceinline__ void sample_f2(const TraceArgs& a, float hx, float lx, float2 hyz, float2 lyz,
+                                          Sample<PolF32>& out, CellPolyF2<NK>& cc) {
+    const GridGeo& g = a.geo;
+    float px = hx + lx;
+    float2 pyz = __fadd2_rn(hyz, lyz);
+    if constexpr (MODE == SAMPLE_CLAMP) {
+        const float cx = fminf(fmaxf(px, 0.0f), g.limf[0]);
+        if (cx != px) { hx = cx; lx = 0.0f; px = cx; }
+        const float cy = fminf(fmaxf(pyz.x, 0.0f), g.limf[1]);
+        if (cy != pyz.x) { hyz.x = cy; lyz.x = 0.0f; pyz.x = cy; }
+        const float cz = fminf(fmaxf(pyz.y, 0.0f), g.limf[2]);
+        if (cz != pyz.y) { hyz.y = cz; lyz.y = 0.0f; pyz.y = cz; }
+    }
+    int ix, iy, iz;
+    if constexpr (MODE != SAMPLE_INTERIOR) {
+        const bool in = (px >= 0.0f) & (px <= g.limf[0]) & (pyz.x >= 0.0f) & (pyz.x <= g.limf[1]) &
+                        (pyz.y >= 0.0f) & (pyz.y <= g.limf[2]);
+        if (!in) {
+            out.q = out.g0 = out.g1 = out.g2 = out.k = 0.0f;
+            return;
+        }
+        ix = min((int)px, g.n[0] - 2);
+        iy = min((int)pyz.x, g.n[1] - 2);
+        iz = min((int)pyz.y, g.n[2] - 2);
+    } else {
+        ix = (int)min((unsigned)(int)px, (unsigned)(g.n[0] - 2));
+        iy = (int)min((unsigned)(int)pyz.x, (unsigned)(g.n[1] - 2));
+        iz = (int)min((unsigned)(int)pyz.y, (unsigned)(g.n[2] - 2));
+    }
+    const float fx = (hx - (float)ix) + lx;
+    const float2 fyz = __fadd2_rn(__fadd2_rn(hyz, make_float2(-(float)iy, -(float)iz)), lyz);
+    const unsigned b = (unsigned)ix * g.sx + (unsigned)iy * g.sy + (unsigned)iz;
+    if (b != cc.base) paired_fill<PolF32, IB>(a, b, cc);
+    const float2 fx2 = bc2(fx), fy2 = bc2(fyz.x), fz2 = bc2(fyz.y);
+    const float2 r0 = poly_eval2(cc.t[0], fx2, fy2, fz2);
+    const float2 r1 = poly_eval2(cc.t[1], fx2, fy2, fz2);
+    out.q = r0.x;
+    out.g0 = r0.y;
+    out.g1 = r1.x;
+    out.g2 = r1.y;
+    if constexpr (IB == IB_SUBCRITICAL) {
+        out.k = poly_eval<float>(cc.k, fx, fyz.x, fyz.y) * a.cl_lof;
+    } else if constexpr (IB == IB_GENERAL) {
+        out.k = poly_eval<float>(cc.k, fx, fyz.x, fyz.y);
+    } else {
+        out.k = 0.0f;
+    }
+}
+
+// s + x with the compensation c (AccF::add on a pair)
+__device__ __forceinline__ void kahan2(float2& s, float2& c, float2 x) {
+    const float2 y = __fadd2_rn(x, c);
+    const float2 t = __fadd2_rn(s, y);
+    c = __fadd2_rn(y, __ffma2_rn(s, bc2(1.0f), make_float2(-t.x, -t.y)) );
+    s = t;
+}
+
+template <int IB, bool SMALLX, int MODE, int NK>
+__device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, CellPolyF2<NK>& cc, float phi) {
+    const float two = 2.0f;
+    const float hphi = 0.5f * phi, phi6 = phi * (1.0f / 6.0f), phi2_6 = phi * phi6;
+    const float S0 = a.Sf[0];
+    const float2 S12 = make_float2(a.Sf[1], a.Sf[2]);
+    const float ope2 = a.ope2f;
+    const float2 hphi2 = bc2(hphi), two2 = bc2(two);
+    const float phx = r.p[0].s, plx = r.p[0].c, wex = r.w[0].s + r.w[0].c;
+    const float2 phyz = make_float2(r.p[1].s, r.p[2].s), plyz = make_float2(r.p[1].c, r.p[2].c);
+    const float2 weyz = __fadd2_rn(make_float2(r.w[1].s, r.w[2].s), make_float2(r.w[1].c, r.w[2].c));
+    constexpr bool kPairPhase = SMALLX;
+    Sample<PolF32> s;
+    // stage 1 at p
+    sample_f2<IB, MODE>(a, phx, plx, phyz, plyz, s, cc);
+    float g = 0.0f, q1 = 0.0f, q3 = 0.0f;
+    if constexpr (kPairPhase) q1 = s.q; else g = nm1<PolF32, SMALLX>(ope2 * s.q);
+    float kq = s.k;
+    float sAx = S0 * s.g0;
+    float2 sAyz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
+    float sWx = sAx;
+    float2 sWyz = sAyz;
+    // stage 2 at p + phi*w/2
+    float stx = plx + hphi * wex;
+    float2 styz = __ffma2_rn(hphi2, weyz, plyz);
+    sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
+    stx = plx + hphi * (wex + hphi * sAx);                        // p + phi*w2/2
+    styz = __ffma2_rn(hphi2, __ffma2_rn(hphi2, sAyz, weyz), plyz);
+    float w3x;
+    float2 w3yz;
+    {
+        const float Ax = S0 * s.g0;
+        const float2 Ayz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
+        w3x = wex + hphi * Ax;
+        w3yz = __ffma2_rn(hphi2, Ayz, weyz);
+        sAx += Ax;
+        sAyz = __fadd2_rn(sAyz, Ayz);
+        sWx += two * Ax;
+        sWyz = __ffma2_rn(two2, Ayz, sWyz);
+    }
+    if constexpr (kPairPhase) {
+        const float2 n12 = nm1_series2(__fmul2_rn(bc2(ope2), make_float2(q1, s.q)));
+        g = n12.x + two * n12.y;
+    } else {
+        g += two * nm1<PolF32, SMALLX>(ope2 * s.q);
+    }
+    kq += two * s.k;
+    // stage 3 at p + phi*w2/2
+    sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
+    {
+        const float Ax = S0 * s.g0;
+        const float2 Ayz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
+        sAx += Ax;
+        sAyz = __fadd2_rn(sAyz, Ayz);
+        sWx += two * Ax;
+        sWyz = __ffma2_rn(two2, Ayz, sWyz);
+        stx = plx + phi * w3x;
+        styz = __ffma2_rn(bc2(phi), w3yz, plyz);
+    }
+    if constexpr (kPairPhase) q3 = s.q; else g += two * nm1<PolF32, SMALLX>(ope2 * s.q);
+    kq += two * s.k;
+    // stage 4 at p + phi*w3
+    sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
+    sWx += S0 * s.g0;
+    sWyz = __ffma2_rn(S12, make_float2(s.g1, s.g2), sWyz);
+    if constexpr (kPairPhase) {
+        const float2 n34 = nm1_series2(__fmul2_rn(bc2(ope2), make_float2(q3, s.q)));
+        g += two * n34.x + n34.y;
+    } else {
+        g += nm1<PolF32, SMALLX>(ope2 * s.q);
+    }
+    kq += s.k;
+    // x: the scalar update
+    r.p[0].add(phi * r.w[0].hi() + (phi * r.w[0].lo() + phi2_6 * sAx));
+    r.w[0].add(phi6 * sWx);
+    // y, z: the same update on pairs
+    {
+        const float2 phi2 = bc2(phi);
+        const float2 whi = make_float2(r.w[1].s, r.w[2].s), wlo = make_float2(r.w[1].c, r.w[2].c);
+        const float2 dp = __ffma2_rn(phi2, whi, __ffma2_rn(phi2, wlo, __fmul2_rn(bc2(phi2_6), sAyz)));
+        float2 ps = phyz, pc = plyz;
+        kahan2(ps, pc, dp);
+        r.p[1].s = ps.x; r.p[2].s = ps.y; r.p[1].c = pc.x; r.p[2].c = pc.y;
+        float2 ws = whi, wc = wlo;
+        kahan2(ws, wc, __fmul2_rn(bc2(phi6), sWyz));
+        r.w[1].s = ws.x; r.w[2].s = ws.y; r.w[1].c = wc.x; r.w[2].c = wc.y;
+    }
+    r.ph += (double)(phi * g);
+    if constexpr (IB != IB_OFF) r.tau.add(phi * kq);
+}
+
+// One RK4 step: the paired FP32 form with the paired cell cache, the generic
+// form otherwise.
+template <class P, int IB, bool SMALLX, int MODE, class Cache>
+__device__ __forceinline__ void step_any(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
+    if constexpr (IsPairedCache<Cache>::value && SLOTH_PAIRED_STEP) {
+        rk4_step_f2<IB, SMALLX, MODE>(a, r, cc, phi);
+    } else {
+        rk4_step<P, IB, SMALLX, MODE>(a, r, cc, phi);
+    }
 }
 
 // Kind of the next step of a ray: 0 plain step of a ray inside the grid whose
@@ -784,11 +963,11 @@ __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, 
             typename P::R phi;
             const int kind = step_kind<P>(a, r, phi);
             if (FAST && kind == 0) {
-                rk4_step<P, IB, SMALLX, SAMPLE_INTERIOR>(a, r, cc, typename P::R(1));
+                step_any<P, IB, SMALLX, SAMPLE_INTERIOR>(a, r, cc, typename P::R(1));
             } else if (kind == 0 || kind == 3) {
-                rk4_step<P, IB, SMALLX, SAMPLE_PLAIN>(a, r, cc, typename P::R(1));
+                step_any<P, IB, SMALLX, SAMPLE_PLAIN>(a, r, cc, typename P::R(1));
             } else {
-                rk4_step<P, IB, SMALLX, SAMPLE_CLAMP>(a, r, cc, phi);
+                step_any<P, IB, SMALLX, SAMPLE_CLAMP>(a, r, cc, phi);
                 if (kind == 2) {
                     r.exited = true;
                     r.lag = 1.0 - (double)phi;
