@@ -45,6 +45,8 @@ constexpr int kAdjThreads = 256;
 // The FP32 backward fits in 128 registers (two 256-thread CTAs per SM) with a
 // few bytes of spill; the FP64 one would spill kilobytes, so it keeps one.
 template <class P> constexpr int adj_bwd_min_blocks() { return sizeof(typename P::R) == 4 ? 2 : 1; }
+// The FP32 forward fits three 256-thread CTAs per SM (80 registers) without spilling.
+template <class P> constexpr int adj_fwd_min_blocks() { return sizeof(typename P::R) == 4 ? 3 : 1; }
 constexpr int kMaxCkptEvery = 32;
 constexpr int kMaxTaps = 65;          // 2 * 4 * sigma + 1 pixels at sigma <= 8
 
@@ -496,7 +498,7 @@ __device__ __forceinline__ void splat_adjoint(const ImageArgs& a, double pa, dou
 // Kernels.
 // ---------------------------------------------------------------------------
 template <class P>
-__global__ void __launch_bounds__(kAdjThreads) image_forward_kernel(const __grid_constant__ ImageArgs a) {
+__global__ void __launch_bounds__(kAdjThreads, adj_fwd_min_blocks<P>()) image_forward_kernel(const __grid_constant__ ImageArgs a) {
     using R = typename P::R;
     __shared__ unsigned long long s_steps;
     if (threadIdx.x == 0) s_steps = 0;
