@@ -35,6 +35,7 @@ class Job:
     keep: list = field(default_factory=list)      # buffers the server reads until admission
     out: Optional[dict] = None                    # pinned host results once fetched
     done_at: Optional[float] = None
+    request: Optional[object] = None              # the stream request it serves (replay)
 
 
 class RayServer:
@@ -249,9 +250,12 @@ def replay(server: RayServer, requests, *, L=5e-3, lwl=532e-9, Te=20.0, Z=1.0, w
     i = 0
     live = []
     lat, steps = [], 0
+    records = []           # (arrival s, grid n, rays, latency s) per request, in completion order
+    loop_max = 0.0
     first = None
     while i < len(requests) or live:
-        now = time.perf_counter() - t0
+        loop_start = time.perf_counter()
+        now = loop_start - t0
         while i < len(requests) and (not realtime or requests[i].t <= now):
             r = requests[i]
             rays = workloads.gaussian_beam(r.rays, waist=waist, L=L, seed=r.ray_seed, device="cuda")
@@ -260,6 +264,7 @@ def replay(server: RayServer, requests, *, L=5e-3, lwl=532e-9, Te=20.0, Z=1.0, w
             job = server.submit(k, fields[k], (-L / 2,) * 3, (h(r.n),) * 3, (r.n,) * 3, rays, lwl=lwl,
                                 detector_plane=L / 2, inv_brems=kol, Te=Te, Z=Z,
                                 arrival=t0 + (r.t if realtime else 0.0))
+            job.request = r
             live.append(job)
             first = first if first is not None else job.arrival
             i += 1
@@ -273,11 +278,14 @@ def replay(server: RayServer, requests, *, L=5e-3, lwl=532e-9, Te=20.0, Z=1.0, w
             elif st == capi.SLOTH_JOB_FETCHED:
                 j.done_at = time.perf_counter()
                 lat.append(j.done_at - j.arrival)
+                rq = getattr(j, "request", None)
+                records.append((j.arrival - t0, rq.n if rq else 0, rq.rays if rq else 0, j.done_at - j.arrival))
                 steps += int(j.out["total_steps"][0])
                 server.release(j)
             else:
                 still.append(j)
         live = still
+        loop_max = max(loop_max, time.perf_counter() - loop_start)
         if time.perf_counter() - t0 > max_seconds:
             raise TimeoutError("request stream did not finish")
     t_end = time.perf_counter()
@@ -285,4 +293,4 @@ def replay(server: RayServer, requests, *, L=5e-3, lwl=532e-9, Te=20.0, Z=1.0, w
     return {"latency_s": lat, "p50_ms": float(np.percentile(lat, 50) * 1e3),
             "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
             "ray_steps": steps, "seconds": t_end - first, "ray_steps_per_s": steps / (t_end - first),
-            "requests": len(lat), "stats": server.stats()}
+            "requests": len(lat), "stats": server.stats(), "records": records, "host_loop_max_ms": loop_max * 1e3}
