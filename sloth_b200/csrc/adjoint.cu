@@ -621,14 +621,12 @@ __device__ __forceinline__ double stencil_t(const void* gg, size_t v, int j, int
 
 template <class P, class Out>
 __global__ void __launch_bounds__(256) pack_adjoint_kernel(const void* __restrict__ gg, Out* __restrict__ out,
-                                                           GridGeo g, double scale, long long total) {
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < total; v += stride) {
-        const int k = (int)(v % g.n[2]);
-        const long long t = v / g.n[2];
-        const int j = (int)(t % g.n[1]);
-        const int i = (int)(t / g.n[1]);
-        const size_t vi = (size_t)v;
+                                                           GridGeo g, double scale) {
+  // x over k (coalesced), y over j, z over i, as the pack kernel
+  for (int i = blockIdx.z; i < g.n[0]; i += gridDim.z)
+    for (int j = blockIdx.y; j < g.n[1]; j += gridDim.y)
+      for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.n[2]; k += gridDim.x * blockDim.x) {
+        const size_t vi = ((size_t)i * g.n[1] + j) * g.n[2] + k;
         double self[4];
         load_gg<P>(gg, vi, self);
         double r = self[0];
@@ -636,7 +634,7 @@ __global__ void __launch_bounds__(256) pack_adjoint_kernel(const void* __restric
         r += stencil_t<P>(gg, vi, j, g.n[1], g.sy, 2);
         r += stencil_t<P>(gg, vi, k, g.n[2], 1, 3);
         out[vi] = (Out)(r * scale);
-    }
+      }
 }
 
 // ---------------------------------------------------------------------------
@@ -795,11 +793,9 @@ static int pack_adjoint_impl(const SlothGridDesc* g, const void* grid_grad, doub
     if (((uintptr_t)grid_grad & 15u) || ((uintptr_t)ne_grad & (sizeof(Out) - 1))) return SLOTH_ERR_MISALIGNED;
     int sms = 148;
     if ((rc = device_sm_count(&sms)) != SLOTH_OK) return rc;
-    const long long total = (long long)g->n[0] * g->n[1] * g->n[2];
-    long long blocks = (total + 255) / 256;
-    if (blocks > (long long)sms * 16) blocks = (long long)sms * 16;
-    pack_adjoint_kernel<P, Out><<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(grid_grad, ne_grad,
-                                                                                   make_geo(g), ne_scale, total);
+    const dim3 grid((unsigned)((g->n[2] + 255) / 256), (unsigned)(g->n[1] < 65535 ? g->n[1] : 65535),
+                    (unsigned)(g->n[0] < 65535 ? g->n[0] : 65535));
+    pack_adjoint_kernel<P, Out><<<grid, 256, 0, (cudaStream_t)stream>>>(grid_grad, ne_grad, make_geo(g), ne_scale);
     note_launch();
     return cuda_status(cudaGetLastError());
 }

@@ -19,16 +19,16 @@ __device__ __forceinline__ double qat(const In* __restrict__ ne, size_t i, doubl
     return __dmul_rn((double)__ldg(ne + i), scale);
 }
 
+// Launch shape: x over k (contiguous, coalesced), y over j, z over i, each
+// axis strided when the grid has more points than the launch dimension; no
+// index arithmetic beyond a multiply-add per voxel.
 template <class In, bool F64OUT>
 __global__ void __launch_bounds__(256) pack_kernel(const In* __restrict__ ne, void* __restrict__ out,
-                                                   GridGeo g, double scale, long long total) {
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < total; v += stride) {
-        const int k = (int)(v % g.n[2]);
-        const long long t = v / g.n[2];
-        const int j = (int)(t % g.n[1]);
-        const int i = (int)(t / g.n[1]);
-        const size_t vi = (size_t)v;
+                                                   GridGeo g, double scale) {
+  for (int i = blockIdx.z; i < g.n[0]; i += gridDim.z)
+    for (int j = blockIdx.y; j < g.n[1]; j += gridDim.y)
+      for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.n[2]; k += gridDim.x * blockDim.x) {
+        const size_t vi = ((size_t)i * g.n[1] + j) * g.n[2] + k;
         const double q = qat(ne, vi, scale);
         double d0, d1, d2;
         if (i == 0)               d0 = qat(ne, vi + g.sx, scale) - q;
@@ -47,7 +47,13 @@ __global__ void __launch_bounds__(256) pack_kernel(const In* __restrict__ ne, vo
         } else {
             reinterpret_cast<float4*>(out)[vi] = make_float4((float)q, (float)d0, (float)d1, (float)d2);
         }
-    }
+      }
+}
+
+// Launch shape of the grid-wide voxel kernels (pack, pack adjoint).
+inline dim3 voxel_grid(const SlothGridDesc* gd) {
+    return dim3((unsigned)((gd->n[2] + 255) / 256), (unsigned)(gd->n[1] < 65535 ? gd->n[1] : 65535),
+                (unsigned)(gd->n[0] < 65535 ? gd->n[0] : 65535));
 }
 
 template <class P>
@@ -93,11 +99,12 @@ static int pack_impl(const SlothGridDesc* g, const void* ne, int ne_is_f64, doub
     const GridGeo geo = make_geo(g);
     const long long total = (long long)g->n[0] * g->n[1] * g->n[2];
     cudaStream_t s = (cudaStream_t)stream;
-    const int blocks = grid_blocks(total, 16);
+    (void)total;
+    const dim3 grid = voxel_grid(g);
     if (ne_is_f64)
-        pack_kernel<double, F64OUT><<<blocks, 256, 0, s>>>((const double*)ne, grid_out, geo, ne_scale, total);
+        pack_kernel<double, F64OUT><<<grid, 256, 0, s>>>((const double*)ne, grid_out, geo, ne_scale);
     else
-        pack_kernel<float, F64OUT><<<blocks, 256, 0, s>>>((const float*)ne, grid_out, geo, ne_scale, total);
+        pack_kernel<float, F64OUT><<<grid, 256, 0, s>>>((const float*)ne, grid_out, geo, ne_scale);
     note_launch();
     return cuda_status(cudaGetLastError());
 }
