@@ -170,6 +170,33 @@ __device__ __forceinline__ bool locate(const GridGeo& g, const typename P::R (&h
     return true;
 }
 
+// FP32: the gradient channels as two polynomial pairs, (q, dq/du) and
+// (dq/dv, dq/dw), in the float4 voxel's own register pairs, evaluated with
+// sm_100's paired FP32 instructions (q is carried along at no cost).
+struct GradCellF2 {
+    unsigned base;
+    float2 t[2][8];
+};
+
+__device__ __forceinline__ void load_cell_f2(const ImageArgs& a, unsigned b, GradCellF2& cc) {
+    if (b == cc.base) return;
+    cc.base = b;
+    const GridGeo& g = a.geo;
+    const float4* gp = reinterpret_cast<const float4*>(a.grid);
+    const float4 v0 = __ldg(gp + b), v1 = __ldg(gp + b + 1u);
+    const float4 v2 = __ldg(gp + b + g.sy), v3 = __ldg(gp + b + g.sy + 1u);
+    const float4 v4 = __ldg(gp + b + g.sx), v5 = __ldg(gp + b + g.sx + 1u);
+    const float4 v6 = __ldg(gp + b + g.sx + g.sy), v7 = __ldg(gp + b + g.sx + g.sy + 1u);
+#define SLOTH_LO(v) make_float2(v.x, v.y)
+#define SLOTH_HI(v) make_float2(v.z, v.w)
+    poly_coeffs2(cc.t[0], SLOTH_LO(v0), SLOTH_LO(v1), SLOTH_LO(v2), SLOTH_LO(v3), SLOTH_LO(v4), SLOTH_LO(v5),
+                 SLOTH_LO(v6), SLOTH_LO(v7));
+    poly_coeffs2(cc.t[1], SLOTH_HI(v0), SLOTH_HI(v1), SLOTH_HI(v2), SLOTH_HI(v3), SLOTH_HI(v4), SLOTH_HI(v5),
+                 SLOTH_HI(v6), SLOTH_HI(v7));
+#undef SLOTH_LO
+#undef SLOTH_HI
+}
+
 template <class P>
 __device__ __forceinline__ void load_cell(const ImageArgs& a, unsigned b, GradCell<P>& cc) {
     using R = typename P::R;
@@ -186,9 +213,9 @@ __device__ __forceinline__ void load_cell(const ImageArgs& a, unsigned b, GradCe
 }
 
 // Acceleration S * grad(q) at hi + lo (zero outside).
-template <class P>
+template <class P, class Cell>
 __device__ __forceinline__ void accel(const ImageArgs& a, const typename P::R (&hi)[3], const typename P::R (&lo)[3],
-                                      typename P::R (&A)[3], GradCell<P>& cc) {
+                                      typename P::R (&A)[3], Cell& cc) {
     using R = typename P::R;
     unsigned b;
     R f[3];
@@ -196,16 +223,25 @@ __device__ __forceinline__ void accel(const ImageArgs& a, const typename P::R (&
         A[0] = A[1] = A[2] = R(0);
         return;
     }
-    load_cell<P>(a, b, cc);
+    if constexpr (std::is_same<Cell, GradCellF2>::value) {
+        load_cell_f2(a, b, cc);
+        const float2 fx = make_float2(f[0], f[0]), fy = make_float2(f[1], f[1]), fz = make_float2(f[2], f[2]);
+        const float2 r0 = poly_eval2(cc.t[0], fx, fy, fz), r1 = poly_eval2(cc.t[1], fx, fy, fz);
+        A[0] = (R)a.S[0] * r0.y;
+        A[1] = (R)a.S[1] * r1.x;
+        A[2] = (R)a.S[2] * r1.y;
+    } else {
+        load_cell<P>(a, b, cc);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) A[k] = (R)a.S[k] * poly_eval<R>(cc.t[k], f[0], f[1], f[2]);
+        for (int k = 0; k < 3; ++k) A[k] = (R)a.S[k] * poly_eval<R>(cc.t[k], f[0], f[1], f[2]);
+    }
 }
 
 // One RK4 step (the tracer's rk4_step with phi = 1, without phase and depth):
 //   p' = p + w + (A1 + A2 + A3)/6,  w' = w + (A1 + 2A2 + 2A3 + A4)/6,
 //   stages at p, p + w/2, p + w/2 + A1/4, p + w + A2/2.
-template <class P>
-__device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, GradCell<P>& cc,
+template <class P, class Cell>
+__device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, Cell& cc,
                                            typename P::R* A1out = nullptr, typename P::R* A2out = nullptr) {
     using R = typename P::R;
     R ph[3], pl[3], we[3], st[3], A1[3], A2[3], A3[3], A4[3];
@@ -252,6 +288,9 @@ struct CornerAcc {
 
 constexpr unsigned kNone = 0xffffffffu;
 
+template <class P> struct AdjTypes { using Cell = GradCell<P>; using Acc = CornerAcc<P>; };
+template <> struct AdjTypes<PolF32> { using Cell = GradCellF2; using Acc = CornerAcc<PolF32>; };
+
 template <class P>
 __device__ __forceinline__ void flush(const ImageArgs& a, CornerAcc<P>& acc) {
     using R = typename P::R;
@@ -272,6 +311,54 @@ __device__ __forceinline__ void flush(const ImageArgs& a, CornerAcc<P>& acc) {
         }
     }
     acc.base = kNone;
+}
+
+// Stage adjoint on the paired FP32 cache with scalar arithmetic (the backward
+// is latency-bound: paired instructions did not shorten it).
+template <class P>
+__device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const float (&hi)[3], const float (&lo)[3],
+                                              const float (&Abar)[3], float (&q)[3], GradCellF2& cc,
+                                              CornerAcc<PolF32>& acc) {
+    unsigned b;
+    float f[3];
+    if (!locate<P>(a.geo, hi, lo, b, f)) {
+        q[0] = q[1] = q[2] = 0.0f;
+        return;
+    }
+    load_cell_f2(a, b, cc);
+    const float fx = f[0], fy = f[1], fz = f[2];
+    float gb[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) gb[k] = (float)a.S[k] * Abar[k];
+    q[0] = q[1] = q[2] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        // channel k + 1 of the voxel: pair k == 0 ? 0 : 1, half k == 0 ? y : (k == 1 ? x : y)
+        float t[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) t[i] = k == 0 ? cc.t[0][i].y : (k == 1 ? cc.t[1][i].x : cc.t[1][i].y);
+        const float dx = (t[1] + fy * t[4]) + fz * (t[5] + fy * t[7]);
+        const float dy = (t[2] + fx * t[4]) + fz * (t[6] + fx * t[7]);
+        const float dz = (t[3] + fx * t[5]) + fy * (t[6] + fx * t[7]);
+        q[0] += gb[k] * dx;
+        q[1] += gb[k] * dy;
+        q[2] += gb[k] * dz;
+    }
+    if (b != acc.base) {
+        flush(a, acc);
+        acc.base = b;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc.v[k][c] = 0.0f;
+    }
+    const float ex = 1.0f - fx, ey = 1.0f - fy, ez = 1.0f - fz;
+    const float w00 = ex * ey, w01 = ex * fy, w10 = fx * ey, w11 = fx * fy;
+    const float w[8] = {w00 * ez, w00 * fz, w01 * ez, w01 * fz, w10 * ez, w10 * fz, w11 * ez, w11 * fz};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc.v[k][c] += gb[k] * w[c];
 }
 
 // Stage adjoint: with Abar = d L / d(stage acceleration), adds
@@ -325,11 +412,11 @@ __device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const typename
 
 // Reverse of model_step from the step's input state r: (lp, lw) = adjoint of
 // the output (p', w') on entry, of the input (p, w) on return.
-template <class P>
+template <class P, class Cell, class Acc>
 __device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const MState<P>& r,
                                                    const typename P::R (&A1)[3], const typename P::R (&A2)[3],
-                                                   typename P::R (&lp)[3], typename P::R (&lw)[3], GradCell<P>& cc,
-                                                   CornerAcc<P>& acc) {
+                                                   typename P::R (&lp)[3], typename P::R (&lw)[3], Cell& cc,
+                                                   Acc& acc) {
     using R = typename P::R;
     R ph[3], pl[3], we[3], st[3];
 #pragma unroll
@@ -514,7 +601,7 @@ __global__ void __launch_bounds__(kAdjThreads, adj_fwd_min_blocks<P>()) image_fo
             r.p[x].set(((double)rays[x * a.n + id] - a.origin[x]) * a.inv_h[x]);
             r.w[x].set((double)rays[(3 + x) * a.n + id] * a.w_of_v[x]);
         }
-        GradCell<P> cc;
+        typename AdjTypes<P>::Cell cc;
         cc.base = kNone;
         for (; t < a.n_steps; ++t) {
             if (ray_gone_model<P>(a, r)) break;
@@ -560,9 +647,9 @@ __global__ void __launch_bounds__(kAdjThreads, adj_bwd_min_blocks<P>()) image_ba
     if (lp[0] == R(0) && lp[1] == R(0) && lp[2] == R(0) && lw[0] == R(0) && lw[1] == R(0) && lw[2] == R(0))
         return;
     const int T = a.nsteps[slot];
-    GradCell<P> cc;
+    typename AdjTypes<P>::Cell cc;
     cc.base = kNone;
-    CornerAcc<P> acc;
+    typename AdjTypes<P>::Acc acc;
     acc.base = kNone;
     // a segment's step inputs and their first two stage accelerations
     MState<P> seg[kMaxCkptEvery];
@@ -581,7 +668,7 @@ __global__ void __launch_bounds__(kAdjThreads, adj_bwd_min_blocks<P>()) image_ba
             model_step_adjoint<P>(a, seg[j], A1, A2, lp, lw, cc, acc);
         }
     }
-    flush<P>(a, acc);
+    flush(a, acc);
 }
 
 // d L / d ne from d L / d(packed grid): the transpose of K1's per-axis
