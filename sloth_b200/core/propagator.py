@@ -153,15 +153,6 @@ def _rays_from(beam, domain, batching_message=True):
     assert isinstance(beam, tuple), "\nExpect a tuple of Beam properties if you wish to batch rays."
 
 
-def _rays_tensor(rays, precision, device):
-    dt = torch.float32 if precision == "f32" else torch.float64
-    if isinstance(rays, torch.Tensor):
-        return rays.to(device=device, dtype=dt, non_blocking=True).contiguous()
-    arr = np.asarray(rays)
-    t = torch.from_numpy(np.ascontiguousarray(arr))
-    return t.to(device=device, dtype=dt, non_blocking=True).contiguous()
-
-
 def _ib_params(domain):
     inv_brems = bool(getattr(domain, "inv_brems", False))
     if not inv_brems:
@@ -183,7 +174,8 @@ class RawSolution:
 # ---------------------------------------------------------------------------
 def solve(beam, ScalarDomain, probing_depth, *, parallelise=True, jitted=True, save_points_per_region=2,
           memory_debug=False, lwl=1064e-9, keep_domain=False, return_raw_results=False, verbose=True,
-          precision="f32", detector_plane=None, return_extras=False, device=None, stream=None):
+          precision="f32", detector_plane=None, return_extras=False, device=None, stream=None,
+          chunk_rays=None):
     """Trace rays through the domain to c*t = sqrt(8)*probing_depth (the
     reference's integration end, :616-617) and return (rf, amp, duration).
 
@@ -192,7 +184,11 @@ def solve(beam, ScalarDomain, probing_depth, *, parallelise=True, jitted=True, s
     save_points_per_region > 2 it is stacked (S, 4, N) over the save times
     linspace(0, 1, S)*sqrt(8)*probing_depth/c and amp is None, as in the
     reference. amp = exp(-tau) when ScalarDomain.inv_brems. duration is the
-    wall time of the trace in seconds (numpy float64).
+    wall time of the trace in seconds (numpy float64), including the rays'
+    and results' copies, which overlap it.
+
+    The rays pass through the device in chunks of ``chunk_rays`` (default
+    ``runtime.STREAM_CHUNK_RAYS``); the results do not depend on it.
     """
     omega = physics.omega_of(lwl)
     region_count = getattr(ScalarDomain, "region_count", 1)
@@ -208,35 +204,30 @@ def solve(beam, ScalarDomain, probing_depth, *, parallelise=True, jitted=True, s
     S = int(save_points_per_region)
     taus = np.linspace(0.0, T, S) if S > 1 else np.array([0.0])
     sched = runtime.schedule_times(taus, grid.spacing) if S > 1 else runtime.Schedule(runtime.nominal_step(grid.spacing), 0, 1, 1)
-    r = _rays_tensor(rays, precision, dev)
     project = detector_plane is not None
-    torch.cuda.synchronize(dev)
-    start = time.time()
-    out = runtime.trace(grid, r, sched, axis=axis, project=project,
-                        plane=float(detector_plane) if project else 0.0, inv_brems=inv_brems, Te=Te, Z=Z,
-                        want_state=return_raw_results, stream=stream)
-    torch.cuda.synchronize(dev)
-    duration = np.float64(time.time() - start)
-    if verbose:
-        print("\nCompleted ray trace in", np.round(duration, 3), "seconds.")
-    # results to host memory: every copy queued, then one synchronisation
+    # rays stream through the device in chunks; their host<->device copies
+    # overlap the tracing of the neighbouring chunks
     want = {}
     if return_raw_results:
-        want["state"] = out["state"]
+        want["state"] = "all"
         if inv_brems:
-            want["amp"] = out["amp"]
+            want["amp"] = "all"
     else:
-        want["jones"] = out["jones"][-1] if S <= 2 else out["jones"]
+        want["jones"] = "last" if S <= 2 else "all"
         if S <= 2 and inv_brems:
-            want["amp"] = out["amp"][-1]
+            want["amp"] = "last"
     if return_extras:
-        for k in ("phase", "status", "steps", "total_steps"):
-            want[k] = out[k]
-    host = dict(zip(want, runtime.to_host(*want.values())))
+        want.update(phase="all", status="all", steps="all")
+    host, total_steps, duration = runtime.trace_to_host(
+        grid, rays, sched, want=want, chunk_rays=chunk_rays, axis=axis, project=project,
+        plane=float(detector_plane) if project else 0.0, inv_brems=inv_brems, Te=Te, Z=Z, stream=stream)
+    duration = np.float64(duration)
+    if verbose:
+        print("\nCompleted ray trace in", np.round(duration, 3), "seconds.")
     extras = None
     if return_extras:
         extras = {"phase": host["phase"], "status": host["status"], "steps": host["steps"],
-                  "total_steps": int(host["total_steps"][0]), "precision": precision}
+                  "total_steps": total_steps, "precision": precision}
 
     def ret(*v):
         return (*v, extras) if return_extras else v
@@ -258,10 +249,11 @@ def solve(beam, ScalarDomain, probing_depth, *, parallelise=True, jitted=True, s
 # ---------------------------------------------------------------------------
 def trace_and_save_depths(beam, ScalarDomain, step, depth_max, output_path, *, lwl=1064e-9, jones_components=None,
                           jitted=True, rtol=1e-3, atol=1e-5, verbose=True, precision="f32", return_extras=False,
-                          device=None, stream=None):
+                          device=None, stream=None, chunk_rays=None):
     """Trace rays and save the Jones vector at depths 0, step, ..., depth_max
     (c*t = depth, :1133-1138); returns {'depth_saves', 'jvec',
-    'jones_components'[, 'amplitude']} and optionally pickles it."""
+    'jones_components'[, 'amplitude']} and optionally pickles it. The rays
+    pass through the device in chunks of ``chunk_rays``, as in ``solve``."""
     omega = physics.omega_of(lwl)
     s0 = _rays_from(beam, ScalarDomain)
     if step <= 0 or depth_max <= 0:
@@ -297,10 +289,10 @@ def trace_and_save_depths(beam, ScalarDomain, step, depth_max, output_path, *, l
     dev = runtime.require_device(device)
     grid = device_grid(ScalarDomain, omega, precision=precision, device=dev, stream=stream)
     sched = runtime.schedule_times(depth_saves, grid.spacing)
-    r = _rays_tensor(s0, precision, dev)
-    out = runtime.trace(grid, r, sched, axis=axis, inv_brems=inv_brems, Te=Te, Z=Z, stream=stream)
-    keys = ["jones"] + (["amp"] if inv_brems else []) + (["phase", "status", "steps"] if return_extras else [])
-    host = dict(zip(keys, runtime.to_host(*(out[k] for k in keys))))
+    want = {k: "all" for k in ["jones"] + (["amp"] if inv_brems else []) +
+            (["phase", "status", "steps"] if return_extras else [])}
+    host, _, _ = runtime.trace_to_host(grid, s0, sched, want=want, chunk_rays=chunk_rays, axis=axis,
+                                       inv_brems=inv_brems, Te=Te, Z=Z, stream=stream)
     jones = host["jones"]
     jvec = [np.asarray(jones[j])[comp, :] for j in range(n_saves)]
     result = {'depth_saves': depth_saves, 'jvec': jvec, 'jones_components': comp}

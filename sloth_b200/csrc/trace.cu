@@ -1,5 +1,6 @@
 // K2 (FP32 split) and K3 (FP64 port) tracer entry points: one trace of one
 // ray set through one grid (the device code is in tracer.cuh).
+#include <algorithm>
 #include <mutex>
 
 #include "tracer.cuh"
@@ -25,8 +26,19 @@ trace_kernel(const __grid_constant__ TraceArgs a) {
         __syncthreads();
         const int tile = s_tile;
         if (tile >= a.n_tiles) break;
-        const long long start = (long long)tile * kTile;
-        const int cnt = (int)min((long long)kTile, a.n - start);
+        // Rays that start together in a tile have similar lifetimes, so a
+        // kTile tile runs as kTile / kThreads waves. The queue ends in tiles
+        // of one wave, so the CTAs finish within about one ray lifetime of
+        // each other instead of one tile.
+        long long start;
+        int cnt;
+        if (tile < a.n_big) {
+            start = (long long)tile * kTile;
+            cnt = kTile;
+        } else {
+            start = (long long)a.n_big * kTile + (long long)(tile - a.n_big) * kSmallTile;
+            cnt = (int)min((long long)kSmallTile, a.n - start);
+        }
         trace_tile<P, IB, SMALLX, FAST>(a, start, cnt, s_key, s_id, &s_head, cc, my_steps);
     }
     // one atomic per CTA for the ray-step total
@@ -47,8 +59,14 @@ static int launch_trace_k(const TraceArgs& ta, int sms, cudaStream_t s) {
         if (dev >= 0 && dev < 64) cached[dev] = per_sm;
     }
     long long blocks = (long long)sms * per_sm;
-    if (blocks > ta.n_tiles) blocks = ta.n_tiles;
-    trace_kernel<P, IB, SMALLX, FAST><<<(int)blocks, kThreads, 0, s>>>(ta);
+    // tile queue: big tiles, then the last kTailWaves small tiles per CTA
+    TraceArgs t = ta;
+    const long long small = std::min(ta.n, (long long)kTailWaves * blocks * kSmallTile);
+    t.n_big = (int)((ta.n - small) / kTile);
+    const long long rest = ta.n - (long long)t.n_big * kTile;
+    t.n_tiles = t.n_big + (int)((rest + kSmallTile - 1) / kSmallTile);
+    if (blocks > t.n_tiles) blocks = t.n_tiles;
+    trace_kernel<P, IB, SMALLX, FAST><<<(int)blocks, kThreads, 0, s>>>(t);
     note_launch();
     return cuda_status(cudaGetLastError());
 }

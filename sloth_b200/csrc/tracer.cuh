@@ -86,7 +86,8 @@ struct TraceArgs {
     const unsigned* perm;      // bucket-ordered ray ids
     const unsigned* skeys;     // their keys
     int* tile_counter;
-    int n_tiles;
+    int n_tiles;      // n_big tiles of kTile rays, then tiles of kSmallTile rays
+    int n_big;
     double origin[3], spacing[3];
     double w_of_v[3];          // w = v * w_of_v   (cells per step per m/s)
     double v_of_w[3];          // v = w * v_of_w
@@ -894,11 +895,12 @@ __device__ __forceinline__ bool start_ray(const TraceArgs& a, unsigned id, Ray<P
     return settle<P>(a, r, my_steps);
 }
 
-// Shared-memory bitonic sort of (key, id) pairs, ascending by key then id.
-__device__ __forceinline__ void tile_sort(unsigned* key, unsigned* id) {
-    for (int k = 2; k <= kTile; k <<= 1) {
+// Shared-memory bitonic sort of `size` (a power of two, <= kTile) (key, id)
+// pairs, ascending by key then id. `size` must be the same in every thread.
+__device__ __forceinline__ void tile_sort(unsigned* key, unsigned* id, int size) {
+    for (int k = 2; k <= size; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
+            for (int i = threadIdx.x; i < size; i += blockDim.x) {
                 const int l = i ^ j;
                 if (l > i) {
                     const unsigned ki = key[i], kl = key[l], ii = id[i], il = id[l];
@@ -927,7 +929,9 @@ __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, 
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
+    int size = 32;                      // sort the smallest power of two that holds the tile
+    while (size < cnt) size <<= 1;
+    for (int i = threadIdx.x; i < size; i += blockDim.x) {
         if (i < cnt) {
             s_key[i] = a.skeys[start + i];
             s_id[i] = a.perm[start + i];
@@ -937,7 +941,7 @@ __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, 
         }
     }
     __syncthreads();
-    tile_sort(s_key, s_id);
+    tile_sort(s_key, s_id, size);
 
     Ray<P> r;
     bool active = false, qempty = false;
@@ -1039,39 +1043,80 @@ __global__ void __launch_bounds__(256) keys_kernel(const KeyArgs k) {
     }
 }
 
-// Exclusive scan of nb (<= 2^18) counts by one CTA of 1024 threads.
+// Exclusive scan of nb (<= 2^18) counts by one CTA of 1024 threads, in
+// passes of 16384 counts: each thread takes 16 consecutive counts (four
+// 16-byte loads; hist is 256-byte aligned), the block scans the per-thread
+// sums, and a running carry links the passes. The next pass's counts are
+// loaded before this pass's block scan, so their latency overlaps it.
+constexpr int kScanPer = 16;
+constexpr int kScanPass = 1024 * kScanPer;
+
+__device__ __forceinline__ void scan_load(const unsigned* hist, int nb, int i0, unsigned (&x)[kScanPer]) {
+    if (i0 + kScanPer <= nb) {
+        const uint4* h4 = reinterpret_cast<const uint4*>(hist + i0);
+#pragma unroll
+        for (int q = 0; q < kScanPer / 4; ++q) {
+            const uint4 u = h4[q];
+            x[4 * q] = u.x;
+            x[4 * q + 1] = u.y;
+            x[4 * q + 2] = u.z;
+            x[4 * q + 3] = u.w;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < kScanPer; ++j) x[j] = i0 + j < nb ? hist[i0 + j] : 0u;
+    }
+}
+
 static __global__ void __launch_bounds__(1024) scan_kernel(unsigned* hist, int nb) {
     __shared__ unsigned s_warp[32];
-    const int t = threadIdx.x;
-    const int per = (nb + 1023) / 1024;
-    const int lo = min(t * per, nb), hi = min(lo + per, nb);
-    unsigned sum = 0;
-    for (int i = lo; i < hi; ++i) sum += hist[i];
-    // block exclusive scan of the per-thread sums
-    unsigned inc = sum;
-    const int lane = t & 31, wid = t >> 5;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    unsigned v[kScanPer], nx[kScanPer];
+    scan_load(hist, nb, t * kScanPer, v);
+    unsigned carry = 0;
+    for (int base = 0; base < nb; base += kScanPass) {
+        const int i0 = base + t * kScanPer;
+        if (base + kScanPass < nb) scan_load(hist, nb, i0 + kScanPass, nx);
+        unsigned sum = 0;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += y;
-    }
-    if (lane == 31) s_warp[wid] = inc;
-    __syncthreads();
-    if (wid == 0) {
-        unsigned v = s_warp[lane];
+        for (int j = 0; j < kScanPer; ++j) {
+            const unsigned c = v[j];
+            v[j] = sum;
+            sum += c;
+        }
+        unsigned inc = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const unsigned y = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane >= o) v += y;
+            const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
         }
-        s_warp[lane] = v;
-    }
-    __syncthreads();
-    unsigned run = inc - sum + (wid > 0 ? s_warp[wid - 1] : 0u);
-    for (int i = lo; i < hi; ++i) {
-        const unsigned c = hist[i];
-        hist[i] = run;
-        run += c;
+        if (lane == 31) s_warp[wid] = inc;
+        __syncthreads();
+        if (wid == 0) {
+            unsigned w = s_warp[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            s_warp[lane] = w;
+        }
+        __syncthreads();
+        const unsigned excl = carry + (inc - sum) + (wid > 0 ? s_warp[wid - 1] : 0u);
+        carry += s_warp[31];
+        if (i0 + kScanPer <= nb) {
+            uint4* h4 = reinterpret_cast<uint4*>(hist + i0);
+#pragma unroll
+            for (int q = 0; q < kScanPer / 4; ++q)
+                h4[q] = make_uint4(v[4 * q] + excl, v[4 * q + 1] + excl, v[4 * q + 2] + excl, v[4 * q + 3] + excl);
+        } else {
+#pragma unroll
+            for (int j = 0; j < kScanPer; ++j)
+                if (i0 + j < nb) hist[i0 + j] = v[j] + excl;
+        }
+        __syncthreads();   // s_warp is rewritten by the next pass
+#pragma unroll
+        for (int j = 0; j < kScanPer; ++j) v[j] = nx[j];
     }
 }
 
@@ -1157,6 +1202,7 @@ inline void fill_trace_args(TraceArgs& ta, const SlothGridDesc* g, const void* g
     ta.skeys = skeys;
     ta.tile_counter = nullptr;
     ta.n_tiles = (int)((n + kTile - 1) / kTile);
+    ta.n_big = ta.n_tiles;
     for (int k = 0; k < 3; ++k) {
         const double h = g->spacing[k];
         ta.origin[k] = g->origin[k];

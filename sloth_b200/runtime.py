@@ -118,20 +118,6 @@ def pack_grid(ne, origin, spacing, omega, *, precision="f32", device=None, strea
                       q_max=max(q_max, 0.0) * (1.0 + 1e-6), q_min=min(q_min, 0.0) * (1.0 + 1e-6), ne_max=ne_max)
 
 
-def to_host(*tensors):
-    """Device tensors -> numpy arrays through pinned host buffers (PyTorch's
-    caching host allocator reuses them across calls): asynchronous copies on
-    the current stream, one synchronisation."""
-    outs = []
-    for t in tensors:
-        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-        h.copy_(t, non_blocking=True)
-        outs.append(h)
-    if tensors:
-        torch.cuda.current_stream(tensors[0].device).synchronize()
-    return [h.numpy() for h in outs]
-
-
 def sample(grid: DeviceGrid, points, *, stream=None) -> torch.Tensor:
     """K0: (4, N) interpolated (q, dq/du, dq/dv, dq/dw) at points (3, N) in metres."""
     pts = torch.as_tensor(points, dtype=torch.float64)
@@ -269,3 +255,130 @@ def trace(grid: DeviceGrid, rays: torch.Tensor, sched: Schedule, *, axis=2, proj
     capi.check(fn(grid.desc, capi.ptr(grid.data), p, capi.ptr(rays), n, out, capi.ptr(ws), ws.numel(),
                   _stream_ptr(stream)), "sloth_trace")
     return o
+
+
+_lane_cache: dict = {}
+
+
+def _lanes(dev):
+    """Two side streams of the device (created once) for trace_to_host."""
+    key = str(dev)
+    lanes = _lane_cache.get(key)
+    if lanes is None:
+        lanes = (torch.cuda.Stream(dev), torch.cuda.Stream(dev))
+        _lane_cache[key] = lanes
+    return lanes
+
+
+def _lane_workspace(n: int, dev, lane: int) -> torch.Tensor:
+    need = int(capi.load().sloth_trace_workspace_bytes(n))
+    key = (str(dev), "lane", lane)
+    t = _ws_cache.get(key)
+    if t is None or t.numel() < need:
+        t = torch.empty(need, dtype=torch.uint8, device=dev)
+        _ws_cache[key] = t
+    return t
+
+
+STREAM_CHUNK_RAYS = 1 << 21
+
+
+def trace_to_host(grid: DeviceGrid, rays, sched: Schedule, *, want: dict, chunk_rays: Optional[int] = None,
+                  stream=None, **kw):
+    """Trace rays (6, N) and return the requested outputs as numpy arrays,
+    streaming the rays through the device in chunks.
+
+    ``rays`` is a host or device tensor or a numpy array. ``want`` maps output
+    names ("jones", "state", "phase", "amp", "status", "steps") to "all"
+    (every save) or "last" (the last save; per-ray outputs ignore it). The
+    other keywords are those of ``trace``.
+
+    Chunk c runs on side stream c % 2: its rays are copied in, traced, and
+    its outputs copied into pinned host arrays at the chunk's columns. While
+    one chunk traces, the other stream's copies run, so the host<->device
+    traffic hides under the tracer except for the first chunk's rays and the
+    last chunk's outputs. Each ray's arithmetic does not depend on the other
+    rays of its launch, so the results are bitwise those of one trace of all
+    N rays.
+
+    Returns (dict of numpy arrays, total ray-steps, seconds from the first
+    copy to the last output on the host).
+    """
+    import time
+
+    dtype = torch.float32 if grid.precision == "f32" else torch.float64
+    dev = grid.data.device
+    src = torch.from_numpy(np.ascontiguousarray(rays)) if not isinstance(rays, torch.Tensor) else rays
+    if src.dim() != 2 or src.shape[0] != 6:
+        raise ValueError("rays must have shape (6, N)")
+    if src.stride(1) != 1:
+        src = src.contiguous()
+    n = int(src.shape[1])
+    S = sched.n_saves
+    cs = int(chunk_rays or STREAM_CHUNK_RAYS)
+    n_chunks = max(1, -(-n // cs))
+    cs = -(-n // n_chunks) if n else 0          # equal chunks but the last: the lanes reuse their buffers
+    bounds = [min(n, c * cs) for c in range(n_chunks + 1)]
+    inv_brems = bool(kw.get("inv_brems", False))
+    want = {k: v for k, v in want.items() if k != "amp" or inv_brems}
+
+    def host_shape(k):
+        rows = {"jones": (4,), "state": (6,)}.get(k, ())
+        if k in ("status", "steps"):
+            return (n,)
+        return ((S,) if want[k] == "all" else ()) + rows + (n,)
+
+    hdt = {"jones": dtype, "state": dtype, "amp": dtype, "phase": torch.float64, "status": torch.uint8,
+           "steps": torch.int32}
+    host = {k: torch.empty(host_shape(k), dtype=hdt[k], pin_memory=True) for k in want}
+    totals = torch.empty(n_chunks, dtype=torch.int64, pin_memory=True)
+    cur = stream if stream is not None else torch.cuda.current_stream(dev)
+    ready = torch.cuda.Event()
+    ready.record(cur)
+    lanes = _lanes(dev)
+    for lane in lanes:
+        lane.wait_event(ready)
+    outs = ({}, {})
+    stage = [None, None]
+    t0 = time.perf_counter()
+    for c in range(n_chunks):
+        a, b = bounds[c], bounds[c + 1]
+        li = c % 2
+        lane = lanes[li]
+        with torch.cuda.stream(lane):
+            m = b - a
+            st = stage[li]
+            if st is None or st.shape[1] != m or st.dtype != src.dtype:
+                st = torch.empty((6, m), dtype=src.dtype, device=dev)
+                stage[li] = st
+            for r in range(6):
+                st[r].copy_(src[r, a:b], non_blocking=True)
+            rc = st if src.dtype == dtype else st.to(dtype)
+            o = trace(grid, rc, sched, stream=lane, workspace=_lane_workspace(m, dev, li), outputs=outs[li],
+                      want_state="state" in want, want_phase="phase" in want, want_amp="amp" in want,
+                      want_status="status" in want, want_steps="steps" in want, **kw)
+            for k, h in host.items():
+                d = o[k]
+                if k in ("status", "steps"):
+                    h[a:b].copy_(d, non_blocking=True)
+                    continue
+                if want[k] == "last":
+                    d = d[-1]
+                    if d.dim() == 1:
+                        h[a:b].copy_(d, non_blocking=True)
+                    else:
+                        for r in range(d.shape[0]):
+                            h[r, a:b].copy_(d[r], non_blocking=True)
+                    continue
+                for s_ in range(S):
+                    if d.dim() == 2:
+                        h[s_, a:b].copy_(d[s_], non_blocking=True)
+                    else:
+                        for r in range(d.shape[1]):
+                            h[s_, r, a:b].copy_(d[s_, r], non_blocking=True)
+            totals[c:c + 1].copy_(o["total_steps"], non_blocking=True)
+    for lane in lanes:
+        lane.synchronize()
+        cur.wait_stream(lane)
+    dt = time.perf_counter() - t0
+    return {k: h.numpy() for k, h in host.items()}, int(totals.sum()), dt
