@@ -95,6 +95,8 @@ struct TraceArgs {
     float Sf[3];               // the same, rounded to FP32 once here (the FP32 tracer reads these
                                // instead of converting the doubles inside its loop)
     float ope2f, cl_lof, cl_wf;
+    float accel_bound;         // bound on |acceleration| (cells per step^2) when it permits the
+                               // interior fast path, else 0 (see interior_run)
     double phase_scale;        // (omega/c) * dtau / 6
     double tau_scale;          // kappa_q2 * dtau / 6
     double cl_w, cl_lo;        // Coulomb log below nc, and max(2, cl_w)
@@ -138,6 +140,7 @@ struct Ray {
     double ph;                 // sum of (n-1) stage combinations
     double lag;                // steps between the ray's time and `step` after an exit step
     int step, save_j, next_save;
+    int run;                   // steps ahead that are certainly interior steps (fast path)
     unsigned id;
     bool exited;               // left the grid through a face-clipped step
 };
@@ -753,6 +756,42 @@ __device__ __forceinline__ int step_kind(const TraceArgs& a, const Ray<P>& r, ty
     return phi < R(1) ? 2 : (near ? 1 : 0);
 }
 
+// Number of steps after the current interior step (kind 0) that are certainly
+// kind 0 too, for a trace whose accelerations are bounded by B =
+// a.accel_bound: 31, 7 or 0. From the state (p, w) now, after j steps
+// |w_j - w| <= j B (each step adds a weighted mean of stage accelerations)
+// and |p_j - p - j w| <= B j^2 / 2 (each step moves w_i + (A1 + A2 + A3) / 6),
+// so the position p_j and the prediction p_j + w_j lie within
+// B (j^2 / 2 + j) of the segment from p + w to p + (j + 1) w. If that segment,
+// widened by the bound for j = m plus a rounding slack, keeps kFaceMargin from
+// every face, the next m steps are interior steps, and step_kind need not run
+// for them: the steps take the same path as with it, bit for bit.
+template <class P>
+__device__ __forceinline__ int interior_run(const TraceArgs& a, const Ray<P>& r) {
+    using R = typename P::R;
+    const R B = (R)a.accel_bound;
+    const R margin = R(kFaceMargin) + R(0.25);       // face margin + rounding slack (cells)
+    R p[3], w[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        p[x] = r.p[x].val();
+        w[x] = r.w[x].val();
+    }
+    auto fits = [&](int m) {
+        const R dev = margin + B * R(0.5 * m * m + m);
+        bool ok = true;
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            const R e1 = p[x] + w[x], e2 = p[x] + R(m + 1) * w[x];
+            ok = ok & (fmin(e1, e2) >= dev) & (fmax(e1, e2) <= lim_of<R>(a.geo, x) - dev);
+        }
+        return ok;
+    };
+    if (fits(31)) return 31;
+    if (fits(7)) return 7;
+    return 0;
+}
+
 template <class P>
 __device__ __forceinline__ bool ray_in_grid(const TraceArgs& a, const Ray<P>& r) {
     using R = typename P::R;
@@ -891,6 +930,7 @@ __device__ __forceinline__ bool start_ray(const TraceArgs& a, unsigned id, Ray<P
     r.step = 0;
     r.save_j = 0;
     r.next_save = a.first_save;
+    r.run = 0;
     r.id = id;
     return settle<P>(a, r, my_steps);
 }
@@ -965,7 +1005,15 @@ __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, 
         }
         if (active) {
             typename P::R phi;
-            const int kind = step_kind<P>(a, r, phi);
+            int kind;
+            if (FAST && r.run > 0) {
+                --r.run;
+                kind = 0;
+                phi = typename P::R(1);
+            } else {
+                kind = step_kind<P>(a, r, phi);
+                if (FAST && kind == 0) r.run = interior_run<P>(a, r);
+            }
             if (FAST && kind == 0) {
                 step_any<P, IB, SMALLX, SAMPLE_INTERIOR>(a, r, cc, typename P::R(1));
             } else if (kind == 0 || kind == 3) {
@@ -1189,6 +1237,18 @@ inline int launch_prepass(const SlothGridDesc* g, int axis, const R* rays, long 
     return cuda_status(cudaGetLastError());
 }
 
+// Largest |acceleration| (cells per step^2) the grid's density range allows:
+// max_k |S_k| * (q_max - min(q_min, 0)); infinite when the range is unknown.
+inline double interior_accel_bound(const SlothGridDesc* g, const SlothTraceParams* p) {
+    if (!(p->q_max > 0.0) || !std::isfinite(p->q_min) || !(p->q_min <= p->q_max)) return INFINITY;
+    double smax = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        const double r = p->dtau / g->spacing[k];
+        smax = fmax(smax, 0.5 * r * r);
+    }
+    return smax * (p->q_max - fmin(p->q_min, 0.0));
+}
+
 // Kernel arguments of one trace from the public descriptors.
 inline void fill_trace_args(TraceArgs& ta, const SlothGridDesc* g, const void* grid, const SlothTraceParams* p,
                             const void* rays, long long n, const SlothTraceOutputs* out, const unsigned* perm,
@@ -1220,6 +1280,10 @@ inline void fill_trace_args(TraceArgs& ta, const SlothGridDesc* g, const void* g
     ta.ope2f = (float)ta.ope2;
     ta.cl_lof = (float)ta.cl_lo;
     ta.cl_wf = (float)ta.cl_w;
+    {
+        const double B = interior_accel_bound(g, p);
+        ta.accel_bound = B <= kInteriorAccel ? (float)(B * 1.001) : 0.0f;
+    }
     ta.plane = p->plane;
     ta.first_save = p->first_save;
     ta.save_every = p->n_saves > 1 ? p->save_every : 1;
@@ -1262,13 +1326,7 @@ inline int check_trace_params(const SlothGridDesc* g, const SlothTraceParams* p,
 // (a difference of q over at most one cell), and that is within
 // kInteriorAccel. Needs q_max > 0 (known) and q_min <= q_max.
 inline bool interior_bound_ok(const SlothGridDesc* g, const SlothTraceParams* p) {
-    if (!(p->q_max > 0.0) || !std::isfinite(p->q_min) || !(p->q_min <= p->q_max)) return false;
-    double smax = 0.0;
-    for (int k = 0; k < 3; ++k) {
-        const double r = p->dtau / g->spacing[k];
-        smax = fmax(smax, 0.5 * r * r);
-    }
-    return smax * (p->q_max - fmin(p->q_min, 0.0)) <= kInteriorAccel;
+    return interior_accel_bound(g, p) <= kInteriorAccel;
 }
 
 // Tracer mode of a trace: inverse-bremsstrahlung path and phase form.
