@@ -1003,19 +1003,35 @@ __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, 
             if (qempty) break;
             continue;
         }
+        typename P::R phi = typename P::R(1);
+        int kind = -1;
         if (active) {
-            typename P::R phi;
-            int kind;
             if (FAST && r.run > 0) {
                 --r.run;
                 kind = 0;
-                phi = typename P::R(1);
             } else {
                 kind = step_kind<P>(a, r, phi);
                 if (FAST && kind == 0) r.run = interior_run<P>(a, r);
             }
+        }
+        // Fast path: when every lane takes an interior step, the warp takes
+        // `extra` more of them in a uniform loop, as many as every lane's run
+        // allows before its next save (so no save falls inside the loop and
+        // no lane needs the face test, the refill or settle in between).
+        int extra = 0;
+        if (FAST) {
+            const int mine = kind == 0 ? min(r.run, r.next_save - r.step - 1) : 0;
+            extra = __reduce_min_sync(FULL, mine);
+        }
+        if (active) {
             if (FAST && kind == 0) {
-                step_any<P, IB, SMALLX, SAMPLE_INTERIOR>(a, r, cc, typename P::R(1));
+#pragma unroll 1
+                for (int e = 0;; ++e) {
+                    step_any<P, IB, SMALLX, SAMPLE_INTERIOR>(a, r, cc, typename P::R(1));
+                    if (e == extra) break;
+                    ++r.step;
+                }
+                r.run -= extra;
             } else if (kind == 0 || kind == 3) {
                 step_any<P, IB, SMALLX, SAMPLE_PLAIN>(a, r, cc, typename P::R(1));
             } else {
