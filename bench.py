@@ -549,8 +549,9 @@ def run_sloth(args):
                          "dram_frac": (traffic / (kms / 1e3) / 1e9 / peak) if traffic else None,
                          "note": "achieved = logical gather bytes (4 RK4 stages x 8 corners x 16 B per ray-step); "
                                  "the corners come from a register cell cache and L1, so physical DRAM traffic "
-                                 "(traffic, dram_frac, from ncu) is ~1.6 B per ray-step; the kernel is bound by "
-                                 "instruction issue (ncu summary in profiles/)"},
+                                 "(traffic, dram_frac, from ncu) is ~1.5 B per ray-step; the kernel is bound by "
+                                 "its FP32 pipes: instruction issue at ~59% of peak, FMA pipe ~66% active "
+                                 "(ncu summary in profiles/)"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),
