@@ -95,7 +95,11 @@ serve_kernel(const TraceArgs* __restrict__ table, WorkHeader* hdr, const WorkIte
         const long long start = (long long)s_tile * kTile;
         const int cnt = (int)min((long long)kTile, s_args.n - start);
         unsigned long long my_steps = 0;
-        trace_tile<PolF32, IB, SMALLX, false>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
+        // the job's density range bounds its accelerations: the interior fast path
+        if (s_args.accel_bound > 0.0f)
+            trace_tile<PolF32, IB, SMALLX, true>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
+        else
+            trace_tile<PolF32, IB, SMALLX, false>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
         block_add(my_steps, &s_steps, s_args.total_steps);
     }
 }
