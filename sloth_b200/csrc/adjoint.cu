@@ -70,6 +70,7 @@ struct ImageArgs {
     void* image;                 // forward: the image; backward: d L / d image
     void* ggrad;                 // backward: d L / d(packed grid)
     unsigned long long* total_steps;   // forward: steps of all rays are added here (may be null)
+    const unsigned* accel_bound;       // float bits of max |S_k dq/du_k| over the grid (workspace)
 };
 
 // ---------------------------------------------------------------------------
@@ -150,19 +151,28 @@ struct GradCell {
 // Cell and in-cell coordinates of the point hi + lo (the tracer's split: the
 // cell from the rounded sum, the fractions from (hi - i) + lo). False when
 // the point is outside the grid (fill 0).
-template <class P>
+template <class P, bool INTERIOR = false>
 __device__ __forceinline__ bool locate(const GridGeo& g, const typename P::R (&hi)[3],
                                        const typename P::R (&lo)[3], unsigned& base, typename P::R (&f)[3]) {
     using R = typename P::R;
     R p[3];
 #pragma unroll
     for (int x = 0; x < 3; ++x) p[x] = hi[x] + lo[x];
-    const bool in = (p[0] >= R(0)) & (p[0] <= lim_of<R>(g, 0)) & (p[1] >= R(0)) &
-                    (p[1] <= lim_of<R>(g, 1)) & (p[2] >= R(0)) & (p[2] <= lim_of<R>(g, 2));
-    if (!in) return false;
-    const int ix = min((int)p[0], g.n[0] - 2);
-    const int iy = min((int)p[1], g.n[1] - 2);
-    const int iz = min((int)p[2], g.n[2] - 2);
+    int ix, iy, iz;
+    if constexpr (!INTERIOR) {
+        const bool in = (p[0] >= R(0)) & (p[0] <= lim_of<R>(g, 0)) & (p[1] >= R(0)) &
+                        (p[1] <= lim_of<R>(g, 1)) & (p[2] >= R(0)) & (p[2] <= lim_of<R>(g, 2));
+        if (!in) return false;
+        ix = min((int)p[0], g.n[0] - 2);
+        iy = min((int)p[1], g.n[1] - 2);
+        iz = min((int)p[2], g.n[2] - 2);
+    } else {
+        // a point of an interior step: inside by construction; one unsigned
+        // min per axis keeps the index in the grid all the same
+        ix = (int)min((unsigned)(int)p[0], (unsigned)(g.n[0] - 2));
+        iy = (int)min((unsigned)(int)p[1], (unsigned)(g.n[1] - 2));
+        iz = (int)min((unsigned)(int)p[2], (unsigned)(g.n[2] - 2));
+    }
     f[0] = (hi[0] - (R)ix) + lo[0];
     f[1] = (hi[1] - (R)iy) + lo[1];
     f[2] = (hi[2] - (R)iz) + lo[2];
@@ -213,13 +223,13 @@ __device__ __forceinline__ void load_cell(const ImageArgs& a, unsigned b, GradCe
 }
 
 // Acceleration S * grad(q) at hi + lo (zero outside).
-template <class P, class Cell>
+template <class P, bool INTERIOR, class Cell>
 __device__ __forceinline__ void accel(const ImageArgs& a, const typename P::R (&hi)[3], const typename P::R (&lo)[3],
                                       typename P::R (&A)[3], Cell& cc) {
     using R = typename P::R;
     unsigned b;
     R f[3];
-    if (!locate<P>(a.geo, hi, lo, b, f)) {
+    if (!locate<P, INTERIOR>(a.geo, hi, lo, b, f)) {
         A[0] = A[1] = A[2] = R(0);
         return;
     }
@@ -240,7 +250,7 @@ __device__ __forceinline__ void accel(const ImageArgs& a, const typename P::R (&
 // One RK4 step (the tracer's rk4_step with phi = 1, without phase and depth):
 //   p' = p + w + (A1 + A2 + A3)/6,  w' = w + (A1 + 2A2 + 2A3 + A4)/6,
 //   stages at p, p + w/2, p + w/2 + A1/4, p + w + A2/2.
-template <class P, class Cell>
+template <class P, bool INTERIOR = false, class Cell>
 __device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, Cell& cc,
                                            typename P::R* A1out = nullptr, typename P::R* A2out = nullptr) {
     using R = typename P::R;
@@ -251,16 +261,16 @@ __device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, Cel
         pl[x] = r.p[x].lo();
         we[x] = r.w[x].val();
     }
-    accel<P>(a, ph, pl, A1, cc);
+    accel<P, INTERIOR>(a, ph, pl, A1, cc);
 #pragma unroll
     for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * we[x];
-    accel<P>(a, ph, st, A2, cc);
+    accel<P, INTERIOR>(a, ph, st, A2, cc);
 #pragma unroll
     for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * (we[x] + R(0.5) * A1[x]);
-    accel<P>(a, ph, st, A3, cc);
+    accel<P, INTERIOR>(a, ph, st, A3, cc);
 #pragma unroll
     for (int x = 0; x < 3; ++x) st[x] = pl[x] + (we[x] + R(0.5) * A2[x]);
-    accel<P>(a, ph, st, A4, cc);
+    accel<P, INTERIOR>(a, ph, st, A4, cc);
     if (A1out) {
 #pragma unroll
         for (int x = 0; x < 3; ++x) {
@@ -581,6 +591,93 @@ __device__ __forceinline__ void splat_adjoint(const ImageArgs& a, double pa, dou
     gb = (double)sb * a.norm;
 }
 
+// The tracer's interior-step test on the model state: inside the grid, and
+// the prediction p + w at least kFaceMargin inside on every axis. With every
+// stage acceleration below kInteriorAccel, all four stage points of the step
+// are then inside, and locate needs no grid test.
+template <class P>
+__device__ __forceinline__ bool model_interior(const ImageArgs& a, const MState<P>& r) {
+    using R = typename P::R;
+    const R margin = R(kFaceMargin);
+    bool ok = true;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        const R p = r.p[x].val(), pn = p + r.w[x].val(), lim = lim_of<R>(a.geo, x);
+        ok = ok & (p >= R(0)) & (p <= lim) & (pn >= margin) & (pn <= lim - margin);
+    }
+    return ok;
+}
+
+// Steps after an interior step that are certainly interior too (31, 7 or 0),
+// for accelerations bounded by B; the argument of the tracer's interior_run:
+// j steps on, the position and the prediction lie within B (j^2 / 2 + j) of
+// the segment from p + w to p + (j + 1) w.
+template <class P>
+__device__ __forceinline__ int model_interior_run(const ImageArgs& a, const MState<P>& r, float B) {
+    using R = typename P::R;
+    const R margin = R(kFaceMargin) + R(0.25);
+    R p[3], w[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        p[x] = r.p[x].val();
+        w[x] = r.w[x].val();
+    }
+    auto fits = [&](int m) {
+        const R dev = margin + R(B) * R(0.5 * m * m + m);
+        bool ok = true;
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            const R e1 = p[x] + w[x], e2 = p[x] + R(m + 1) * w[x];
+            ok = ok & (fmin(e1, e2) >= dev) & (fmax(e1, e2) <= lim_of<R>(a.geo, x) - dev);
+        }
+        return ok;
+    };
+    if (fits(31)) return 31;
+    if (fits(7)) return 7;
+    return 0;
+}
+
+// The acceleration bound of the fast path: infinity (no fast path) without one.
+__device__ __forceinline__ float load_accel_bound(const ImageArgs& a) {
+    if (!a.accel_bound) return INFINITY;
+    const float b = __uint_as_float(*a.accel_bound);
+    return b * 1.001f;
+}
+
+// Largest |S_k dq/du_k| over the packed grid's gradient channels. Trilinear
+// interpolation stays within its corners' range, so this bounds every stage
+// acceleration of the model. Non-negative floats order as their bit
+// patterns, so the blocks combine with an unsigned atomicMax; a NaN channel
+// gives infinity (no fast path).
+template <class P>
+__global__ void __launch_bounds__(256) accel_bound_kernel(const void* __restrict__ grid, size_t nvox,
+                                                          double s0, double s1, double s2, unsigned* out) {
+    __shared__ float s_max[8];
+    float m = 0.0f;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nvox; i += (size_t)gridDim.x * blockDim.x) {
+        double g0, g1, g2;
+        if constexpr (sizeof(typename P::R) == 4) {
+            const float4 v = reinterpret_cast<const float4*>(grid)[i];
+            g0 = v.y; g1 = v.z; g2 = v.w;
+        } else {
+            const double* d = reinterpret_cast<const double*>(grid) + 4 * i;
+            g0 = d[1]; g1 = d[2]; g2 = d[3];
+        }
+        const double x = fmax(fabs(s0 * g0), fmax(fabs(s1 * g1), fabs(s2 * g2)));
+        const bool nan = !(g0 == g0) || !(g1 == g1) || !(g2 == g2);
+        const float xf = nan ? INFINITY : __double2float_ru(x);
+        m = xf > m ? xf : m;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int wi = 1; wi < (int)(blockDim.x >> 5); ++wi) m = fmaxf(m, s_max[wi]);
+        atomicMax(out, __float_as_uint(m));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Kernels.
 // ---------------------------------------------------------------------------
@@ -603,10 +700,31 @@ __global__ void __launch_bounds__(kAdjThreads, adj_fwd_min_blocks<P>()) image_fo
         }
         typename AdjTypes<P>::Cell cc;
         cc.base = kNone;
+        const float B = load_accel_bound(a);
+        const bool fast = B <= (float)kInteriorAccel;
+        int run = 0, ck = 0, seg = 0;    // ck: steps to the next checkpoint
         for (; t < a.n_steps; ++t) {
-            if (ray_gone_model<P>(a, r)) break;
-            if (t % a.ckpt_every == 0) store_state<P>(a, t / a.ckpt_every, slot, r);
-            model_step<P>(a, r, cc);
+            bool interior = false;
+            if (run > 0) {
+                // proven interior: inside, so not gone either
+                --run;
+                interior = true;
+            } else {
+                if (ray_gone_model<P>(a, r)) break;
+                if (fast && model_interior<P>(a, r)) {
+                    interior = true;
+                    run = model_interior_run<P>(a, r, B);
+                }
+            }
+            if (ck == 0) {
+                store_state<P>(a, seg++, slot, r);
+                ck = a.ckpt_every;
+            }
+            --ck;
+            if (interior)
+                model_step<P, true>(a, r, cc);
+            else
+                model_step<P>(a, r, cc);
         }
         store_state<P>(a, a.n_seg, slot, r);
         a.nsteps[slot] = t;
@@ -658,6 +776,8 @@ __global__ void __launch_bounds__(kAdjThreads, adj_bwd_min_blocks<P>()) image_ba
         load_state<P>(a, s, slot, r);
         const int j0 = s * a.ckpt_every;
         const int m = min(a.ckpt_every, T - j0);
+        // (the interior fast path does not pay here: the backward is
+        // latency-bound, and the second code path costs it registers)
         for (int j = 0; j < m; ++j) {
             seg[j] = r;
             model_step<P>(a, r, cc, &segA[j][0], &segA[j][3]);
@@ -791,18 +911,21 @@ static void fill_image_args(ImageArgs& a, const SlothGridDesc* g, const void* gr
     a.image = nullptr;
     a.ggrad = nullptr;
     a.total_steps = nullptr;
+    a.accel_bound = nullptr;
 }
 
 struct ImageWs {
     unsigned *hist, *keys, *perm, *skeys;
     void* ckpt;
     int* nsteps;
+    unsigned* bound;    // acceleration bound of the forward (float bits), in the header's second half
 };
 
 static ImageWs carve(void* ws, const SlothImageParams* p, long long n) {
     ImageWs w;
     char* base = reinterpret_cast<char*>(ws);
     const size_t a = align256((size_t)(n > 0 ? n : 1) * 4u);
+    w.bound = reinterpret_cast<unsigned*>(base + kHeaderBytes / 2);
     w.hist = reinterpret_cast<unsigned*>(base + kHeaderBytes);
     w.keys = reinterpret_cast<unsigned*>(base + kHeaderBytes + kHistBytes);
     w.perm = reinterpret_cast<unsigned*>(base + kHeaderBytes + kHistBytes + a);
@@ -811,6 +934,20 @@ static ImageWs carve(void* ws, const SlothImageParams* p, long long n) {
     w.ckpt = c;
     w.nsteps = reinterpret_cast<int*>(c + align256((size_t)(image_n_seg(p) + 1) * 48u * (size_t)(n > 0 ? n : 1)));
     return w;
+}
+
+// The acceleration bound of the interior fast path into the workspace.
+template <class P>
+static int launch_accel_bound(const SlothGridDesc* g, const void* grid, const ImageArgs& a, unsigned* bound, int sms,
+                              cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(bound, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return cuda_status(e);
+    const size_t vox = (size_t)g->n[0] * g->n[1] * g->n[2];
+    const size_t want = (vox + 255) / 256, cap = (size_t)sms * 8;
+    accel_bound_kernel<P><<<(unsigned)(want < cap ? want : cap), 256, 0, s>>>(grid, vox, fabs(a.S[0]), fabs(a.S[1]),
+                                                                               fabs(a.S[2]), bound);
+    note_launch();
+    return cuda_status(cudaGetLastError());
 }
 
 template <class P>
@@ -839,6 +976,8 @@ static int image_forward_impl(const SlothGridDesc* g, const void* grid, const Sl
     fill_image_args(a, g, grid, p, rays, n, w.perm, w.ckpt, w.nsteps);
     a.image = image;
     a.total_steps = total_steps;
+    if ((rc = launch_accel_bound<P>(g, grid, a, w.bound, sms, s)) != SLOTH_OK) return rc;
+    a.accel_bound = w.bound;
     image_forward_kernel<P><<<(unsigned)((n + kAdjThreads - 1) / kAdjThreads), kAdjThreads, 0, s>>>(a);
     note_launch();
     return cuda_status(cudaGetLastError());
