@@ -280,7 +280,26 @@ def _lane_workspace(n: int, dev, lane: int) -> torch.Tensor:
     return t
 
 
-STREAM_CHUNK_RAYS = 1 << 21
+STREAM_CHUNK_RAYS = 1 << 22
+STREAM_END_RAYS = 1 << 19
+
+
+def _chunk_bounds(n: int, cs: int) -> list:
+    """Chunk boundaries of n rays for trace_to_host: about `cs` rays per
+    chunk, but the first and the last chunk hold only STREAM_END_RAYS (when
+    cs is larger), because the first chunk's copy in and the last chunk's
+    copy out are the only copies no trace hides."""
+    if n <= 0:
+        return [0, 0]
+    end = min(cs, STREAM_END_RAYS)
+    if n <= 2 * end + cs:
+        k = max(1, -(-n // cs))
+        c = -(-n // k)
+        return [min(n, i * c) for i in range(k + 1)]
+    mid = n - 2 * end
+    k = -(-mid // cs)
+    c = -(-mid // k)
+    return [0] + [min(n - end, end + i * c) for i in range(k + 1)] + [n]
 
 
 def trace_to_host(grid: DeviceGrid, rays, sched: Schedule, *, want: dict, chunk_rays: Optional[int] = None,
@@ -315,10 +334,8 @@ def trace_to_host(grid: DeviceGrid, rays, sched: Schedule, *, want: dict, chunk_
         src = src.contiguous()
     n = int(src.shape[1])
     S = sched.n_saves
-    cs = int(chunk_rays or STREAM_CHUNK_RAYS)
-    n_chunks = max(1, -(-n // cs))
-    cs = -(-n // n_chunks) if n else 0          # equal chunks but the last: the lanes reuse their buffers
-    bounds = [min(n, c * cs) for c in range(n_chunks + 1)]
+    bounds = _chunk_bounds(n, int(chunk_rays or STREAM_CHUNK_RAYS))
+    n_chunks = len(bounds) - 1
     inv_brems = bool(kw.get("inv_brems", False))
     want = {k: v for k, v in want.items() if k != "amp" or inv_brems}
 
