@@ -86,7 +86,9 @@ typedef struct SlothTraceParams {
                                  known to be >= 0). With q_max it bounds the ray's
                                  acceleration; when that bound keeps every stage point
                                  of an interior step inside the grid, those steps skip
-                                 the per-stage grid test (same results, fewer
+                                 the per-stage grid test, and runs of steps proven
+                                 interior skip the face test (bitwise the same results
+                                 in FP32, within 1e-12 relative in FP64; fewer
                                  instructions). A value above the true minimum is an
                                  error of the caller. */
 } SlothTraceParams;
