@@ -355,7 +355,7 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
         out.g1 = r1.x;
         out.g2 = r1.y;
         if constexpr (IB == IB_SUBCRITICAL) {
-            out.k = poly_eval<float>(cc.k, fx, fy, fz) * a.cl_lof;
+            out.k = poly_eval<float>(cc.k, fx, fy, fz);   // cl_lo is in tau_scale
         } else if constexpr (IB == IB_GENERAL) {
             out.k = poly_eval<float>(cc.k, fx, fy, fz);
         } else {
@@ -386,7 +386,7 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
         out.g1 = poly_eval<R>(cc.t[2], fx, fy, fz);
         out.g2 = poly_eval<R>(cc.t[3], fx, fy, fz);
         if constexpr (IB == IB_SUBCRITICAL) {
-            out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz) * arg_cl_lo<R>(a);
+            out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz);   // cl_lo is in tau_scale
         } else if constexpr (IB == IB_GENERAL) {
             out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz);
         } else {
@@ -437,7 +437,7 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
             R k = R(0);
     #pragma unroll
             for (int i = 0; i < 8; ++i) k += w[i] * (c[i].x * c[i].x);
-            out.k = k * arg_cl_lo<R>(a);
+            out.k = k;   // cl_lo is in tau_scale
         } else if constexpr (IB == IB_GENERAL) {
             R k = R(0);
     #pragma unroll
@@ -600,7 +600,7 @@ __device__ __forceinline__ void sample_f2(const TraceArgs& a, float hx, float lx
     out.g1 = r1.x;
     out.g2 = r1.y;
     if constexpr (IB == IB_SUBCRITICAL) {
-        out.k = poly_eval<float>(cc.k, fx, fyz.x, fyz.y) * a.cl_lof;
+        out.k = poly_eval<float>(cc.k, fx, fyz.x, fyz.y);   // cl_lo is in tau_scale
     } else if constexpr (IB == IB_GENERAL) {
         out.k = poly_eval<float>(cc.k, fx, fyz.x, fyz.y);
     } else {
@@ -1253,6 +1253,13 @@ inline int launch_prepass(const SlothGridDesc* g, int axis, const R* rays, long 
     return cuda_status(cudaGetLastError());
 }
 
+// Tracer mode of a trace: inverse-bremsstrahlung path and phase form.
+inline void trace_mode(const SlothTraceParams* p, int* ib, bool* smallx) {
+    const double xmax = p->q_max > 0.0 ? p->q_max * p->ope_ratio2 : 1e300;
+    *smallx = xmax <= kSmallX;
+    *ib = !p->inv_brems ? IB_OFF : (xmax <= 1.0 ? IB_SUBCRITICAL : IB_GENERAL);
+}
+
 // Largest |acceleration| (cells per step^2) the grid's density range allows:
 // max_k |S_k| * (q_max - min(q_min, 0)); infinite when the range is unknown.
 inline double interior_accel_bound(const SlothGridDesc* g, const SlothTraceParams* p) {
@@ -1289,12 +1296,21 @@ inline void fill_trace_args(TraceArgs& ta, const SlothGridDesc* g, const void* g
         ta.Sf[k] = (float)ta.S[k];
     }
     ta.phase_scale = (p->omega / kC) * p->dtau / 6.0;
-    ta.tau_scale = p->kappa_q2 * p->dtau / 6.0;
+    ta.tau_scale = p->kappa_q2 * p->dtau / 6.0;   // times cl_lo below for the sub-critical mode
     ta.cl_w = p->coulomb_log_w;
     ta.cl_lo = p->coulomb_log_w > 2.0 ? p->coulomb_log_w : 2.0;
     ta.ope2 = p->ope_ratio2;
     ta.ope2f = (float)ta.ope2;
     ta.cl_lof = (float)ta.cl_lo;
+    {
+        // Below the critical density the Coulomb log is the constant cl_lo, so
+        // the sub-critical samples leave it out of kappa and the optical
+        // depth's scale takes it once.
+        int ib;
+        bool smallx;
+        trace_mode(p, &ib, &smallx);
+        if (ib == IB_SUBCRITICAL) ta.tau_scale *= ta.cl_lo;
+    }
     ta.cl_wf = (float)ta.cl_w;
     {
         const double B = interior_accel_bound(g, p);
@@ -1345,11 +1361,5 @@ inline bool interior_bound_ok(const SlothGridDesc* g, const SlothTraceParams* p)
     return interior_accel_bound(g, p) <= kInteriorAccel;
 }
 
-// Tracer mode of a trace: inverse-bremsstrahlung path and phase form.
-inline void trace_mode(const SlothTraceParams* p, int* ib, bool* smallx) {
-    const double xmax = p->q_max > 0.0 ? p->q_max * p->ope_ratio2 : 1e300;
-    *smallx = xmax <= kSmallX;
-    *ib = !p->inv_brems ? IB_OFF : (xmax <= 1.0 ? IB_SUBCRITICAL : IB_GENERAL);
-}
 
 }  // namespace sloth
