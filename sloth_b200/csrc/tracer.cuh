@@ -198,8 +198,21 @@ template <int NK>
 struct CellPolyF2 {
     unsigned base;
     float2 t[2][8];
-    float k[NK == 5 ? 8 : 1];
 };
+
+// The FP32 paired cache keeps the cell's kappa polynomial (NK == 5) in shared
+// memory rather than registers: each thread owns one slot, [2][threads]
+// float4 so that a warp's 16-byte loads do not conflict. This keeps 8 values
+// out of the step's 128-register budget; the coefficients are written once
+// per cell and read once per stage, off the step's critical path.
+static __shared__ float4 s_kappa_coef[2][kThreads];
+
+__device__ __forceinline__ void kappa_store(const float (&k)[8]) {
+    s_kappa_coef[0][threadIdx.x] = make_float4(k[0], k[1], k[2], k[3]);
+    s_kappa_coef[1][threadIdx.x] = make_float4(k[4], k[5], k[6], k[7]);
+}
+
+__device__ __forceinline__ float kappa_eval(float fx, float fy, float fz);
 
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) {
     return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);          // a - b, one rounding
@@ -282,13 +295,23 @@ __device__ __forceinline__ void paired_fill(const TraceArgs& a, unsigned b, Cell
 #undef SLOTH_LO
 #undef SLOTH_HI
     if constexpr (IB == IB_SUBCRITICAL) {
-        poly_coeffs<float>(cc.k, v0.x * v0.x, v1.x * v1.x, v2.x * v2.x, v3.x * v3.x, v4.x * v4.x, v5.x * v5.x,
+        float k[8];
+        poly_coeffs<float>(k, v0.x * v0.x, v1.x * v1.x, v2.x * v2.x, v3.x * v3.x, v4.x * v4.x, v5.x * v5.x,
                            v6.x * v6.x, v7.x * v7.x);
+        kappa_store(k);
     } else if constexpr (IB == IB_GENERAL) {
-        poly_coeffs<float>(cc.k, corner_kappa<P>(a, v0.x), corner_kappa<P>(a, v1.x), corner_kappa<P>(a, v2.x),
+        float k[8];
+        poly_coeffs<float>(k, corner_kappa<P>(a, v0.x), corner_kappa<P>(a, v1.x), corner_kappa<P>(a, v2.x),
                            corner_kappa<P>(a, v3.x), corner_kappa<P>(a, v4.x), corner_kappa<P>(a, v5.x),
                            corner_kappa<P>(a, v6.x), corner_kappa<P>(a, v7.x));
+        kappa_store(k);
     }
+}
+
+__device__ __forceinline__ float kappa_eval(float fx, float fy, float fz) {
+    const float4 a = s_kappa_coef[0][threadIdx.x], b = s_kappa_coef[1][threadIdx.x];
+    const float k[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    return poly_eval<float>(k, fx, fy, fz);
 }
 
 // Trilinear sample of the packed grid (rules of src/core/interpolator.py:79-104:
@@ -355,9 +378,9 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
         out.g1 = r1.x;
         out.g2 = r1.y;
         if constexpr (IB == IB_SUBCRITICAL) {
-            out.k = poly_eval<float>(cc.k, fx, fy, fz);   // cl_lo is in tau_scale
+            out.k = kappa_eval(fx, fy, fz);   // cl_lo is in tau_scale
         } else if constexpr (IB == IB_GENERAL) {
-            out.k = poly_eval<float>(cc.k, fx, fy, fz);
+            out.k = kappa_eval(fx, fy, fz);
         } else {
             out.k = 0.0f;
         }
@@ -600,9 +623,9 @@ __device__ __forceinline__ void sample_f2(const TraceArgs& a, float hx, float lx
     out.g1 = r1.x;
     out.g2 = r1.y;
     if constexpr (IB == IB_SUBCRITICAL) {
-        out.k = poly_eval<float>(cc.k, fx, fyz.x, fyz.y);   // cl_lo is in tau_scale
+        out.k = kappa_eval(fx, fyz.x, fyz.y);   // cl_lo is in tau_scale
     } else if constexpr (IB == IB_GENERAL) {
-        out.k = poly_eval<float>(cc.k, fx, fyz.x, fyz.y);
+        out.k = kappa_eval(fx, fyz.x, fyz.y);
     } else {
         out.k = 0.0f;
     }
