@@ -24,7 +24,7 @@ def _rk4_step(p, w, accel):
 
 
 @pytest.mark.parametrize("mode", ["random", "push", "alternate"])
-@pytest.mark.parametrize("m", [7, 31])
+@pytest.mark.parametrize("m", [3, 7, 15, 31, 63])
 def test_run_envelope_holds(mode, m):
     rng = np.random.default_rng(1 + m)
     B = 0.03
