@@ -68,78 +68,115 @@ def _fn(name: str, precision: str):
     return getattr(capi.load(), f"{name}_{precision}")
 
 
+def _image_forward(ne: torch.Tensor, rays: torch.Tensor, origin, spacing, omega: float, spec: DetectorSpec,
+                   precision: str, stats: Optional[dict]):
+    """K1 + K4 on this process's rays: (image, state the backward needs)."""
+    if precision not in ("f32", "f64"):
+        raise ValueError("precision must be 'f32' or 'f64'")
+    if ne.device.type != "cuda" or rays.device.type != "cuda":
+        raise ValueError("ne and rays must be CUDA tensors")
+    runtime.require_device(ne.device)
+    dt = torch.float32 if precision == "f32" else torch.float64
+    rays = rays.to(dt).contiguous()
+    if rays.dim() != 2 or rays.shape[0] != 6:
+        raise ValueError("rays must be (6, N)")
+    grid = runtime.pack_grid(ne.detach(), origin, spacing, omega, precision=precision, device=ne.device)
+    params = spec.params()
+    n = int(rays.shape[1])
+    ws_bytes = int(capi.load().sloth_image_workspace_bytes(ctypes.byref(params), n))
+    if ws_bytes == 0:
+        raise ValueError("invalid detector spec")
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=ne.device)
+    image = torch.empty(tuple(spec.n_px), dtype=dt, device=ne.device)
+    steps = None
+    if stats is not None:
+        steps = torch.zeros(1, dtype=torch.int64, device=ne.device)
+        stats["ray_steps"] = steps
+    stream = torch.cuda.current_stream(ne.device).cuda_stream
+    capi.check(_fn("sloth_image_forward", precision)(grid.desc, capi.ptr(grid.data), ctypes.byref(params),
+                                                     capi.ptr(rays), n, capi.ptr(image),
+                                                     capi.ptr(steps) if steps is not None else None,
+                                                     capi.ptr(ws), ws_bytes, stream), "sloth_image_forward")
+    # the workspace's ray order refers to `rays`, which the state keeps alive
+    state = dict(grid=grid, ws=ws, ws_bytes=ws_bytes, params=params, n=n, precision=precision,
+                 ne_dtype=ne.dtype, ne_shape=tuple(ne.shape), rays=rays)
+    return image, state
+
+
+def _image_backward(state: dict, grad_image: torch.Tensor) -> torch.Tensor:
+    """K5 + the pack adjoint: d loss / d ne from this process's rays."""
+    grid, precision = state["grid"], state["precision"]
+    dt = torch.float32 if precision == "f32" else torch.float64
+    gi = grad_image.to(dt).contiguous()
+    gg = torch.empty_like(grid.data)
+    stream = torch.cuda.current_stream(gi.device).cuda_stream
+    capi.check(_fn("sloth_image_backward", precision)(grid.desc, capi.ptr(grid.data), ctypes.byref(state["params"]),
+                                                      state["n"], capi.ptr(gi), capi.ptr(gg), capi.ptr(state["ws"]),
+                                                      state["ws_bytes"], stream), "sloth_image_backward")
+    ne_grad = torch.empty(state["ne_shape"], dtype=dt, device=gi.device)
+    capi.check(_fn("sloth_grid_pack_adjoint", precision)(grid.desc, capi.ptr(gg), 1.0 / grid.nc,
+                                                         capi.ptr(ne_grad), stream), "sloth_grid_pack_adjoint")
+    return ne_grad.to(state["ne_dtype"])
+
+
+def _sum_over(t: torch.Tensor, group) -> torch.Tensor:
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM, group=group)
+    return t
+
+
 class DetectorImage(torch.autograd.Function):
-    """image = F(ne): differentiable with respect to ne only."""
+    """image = F(ne): differentiable with respect to ne only.
+
+    With a process group, the rays are sharded over its ranks (each passes
+    its own) and the image is the sum over ranks, so every rank returns the
+    image of all rays. The backward then needs the same d loss / d image on
+    every rank (a loss computed from the summed image), and returns d loss /
+    d ne summed over ranks: the gradient of all rays on every rank. These are
+    the model's only exchanges, one all-reduce each way (an image and a grid);
+    every rank must take part in both."""
 
     @staticmethod
     def forward(ctx, ne: torch.Tensor, rays: torch.Tensor, origin: Sequence[float], spacing: Sequence[float],
-                omega: float, spec: DetectorSpec, precision: str = "f32", stats: Optional[dict] = None):
-        if precision not in ("f32", "f64"):
-            raise ValueError("precision must be 'f32' or 'f64'")
-        if ne.device.type != "cuda" or rays.device.type != "cuda":
-            raise ValueError("ne and rays must be CUDA tensors")
-        runtime.require_device(ne.device)
-        dt = torch.float32 if precision == "f32" else torch.float64
-        rays = rays.to(dt).contiguous()
-        if rays.dim() != 2 or rays.shape[0] != 6:
-            raise ValueError("rays must be (6, N)")
-        grid = runtime.pack_grid(ne.detach(), origin, spacing, omega, precision=precision, device=ne.device)
-        params = spec.params()
-        n = int(rays.shape[1])
-        ws_bytes = int(capi.load().sloth_image_workspace_bytes(ctypes.byref(params), n))
-        if ws_bytes == 0:
-            raise ValueError("invalid detector spec")
-        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=ne.device)
-        image = torch.empty(tuple(spec.n_px), dtype=dt, device=ne.device)
-        steps = None
-        if stats is not None:
-            steps = torch.zeros(1, dtype=torch.int64, device=ne.device)
-            stats["ray_steps"] = steps
-        stream = torch.cuda.current_stream(ne.device).cuda_stream
-        capi.check(_fn("sloth_image_forward", precision)(grid.desc, capi.ptr(grid.data), ctypes.byref(params),
-                                                         capi.ptr(rays), n, capi.ptr(image),
-                                                         capi.ptr(steps) if steps is not None else None,
-                                                         capi.ptr(ws), ws_bytes, stream), "sloth_image_forward")
-        ctx.grid, ctx.ws, ctx.ws_bytes, ctx.params, ctx.n = grid, ws, ws_bytes, params, n
-        ctx.precision, ctx.ne_dtype, ctx.ne_shape = precision, ne.dtype, tuple(ne.shape)
-        ctx.keep = rays      # the workspace's ray order refers to these rays
+                omega: float, spec: DetectorSpec, precision: str = "f32", stats: Optional[dict] = None,
+                group=None):
+        image, state = _image_forward(ne, rays, origin, spacing, omega, spec, precision, stats)
+        ctx.state, ctx.group = state, group
+        if group is not None:
+            _sum_over(image, group)
         return image
 
     @staticmethod
     def backward(ctx, grad_image: torch.Tensor):
-        grid, precision = ctx.grid, ctx.precision
-        dt = torch.float32 if precision == "f32" else torch.float64
-        gi = grad_image.to(dt).contiguous()
-        gg = torch.empty_like(grid.data)
-        stream = torch.cuda.current_stream(gi.device).cuda_stream
-        capi.check(_fn("sloth_image_backward", precision)(grid.desc, capi.ptr(grid.data), ctypes.byref(ctx.params),
-                                                          ctx.n, capi.ptr(gi), capi.ptr(gg), capi.ptr(ctx.ws),
-                                                          ctx.ws_bytes, stream), "sloth_image_backward")
-        ne_grad = torch.empty(ctx.ne_shape, dtype=dt, device=gi.device)
-        capi.check(_fn("sloth_grid_pack_adjoint", precision)(grid.desc, capi.ptr(gg), 1.0 / grid.nc,
-                                                             capi.ptr(ne_grad), stream), "sloth_grid_pack_adjoint")
-        return ne_grad.to(ctx.ne_dtype), None, None, None, None, None, None, None
+        ne_grad = _image_backward(ctx.state, grad_image)
+        if ctx.group is not None:
+            _sum_over(ne_grad, ctx.group)
+        return ne_grad, None, None, None, None, None, None, None, None
 
 
 def detector_image(ne: torch.Tensor, rays: torch.Tensor, spec: DetectorSpec, *, origin, spacing,
                    lwl: Optional[float] = None, omega: Optional[float] = None,
-                   precision: str = "f32", stats: Optional[dict] = None) -> torch.Tensor:
+                   precision: str = "f32", stats: Optional[dict] = None, group=None) -> torch.Tensor:
     """The detector image of `rays` (6, N) through the density `ne` (m^-3);
     differentiable with respect to `ne`. If `stats` is a dict, its
-    "ray_steps" entry receives a device counter of the RK4 steps taken."""
+    "ray_steps" entry receives a device counter of the RK4 steps taken (this
+    process's rays). With a torch.distributed process group, each rank passes
+    its share of the rays and gets the image and the gradient of all of them
+    (see DetectorImage)."""
     if omega is None:
         if lwl is None:
             raise ValueError("give lwl or omega")
         omega = physics.omega_of(lwl)
     return DetectorImage.apply(ne, rays, tuple(map(float, origin)), tuple(map(float, spacing)), float(omega),
-                               spec, precision, stats)
+                               spec, precision, stats, group)
 
 
 def image_loss_grad(ne: torch.Tensor, rays: torch.Tensor, target: torch.Tensor, spec: DetectorSpec, *, origin,
-                    spacing, lwl: float, precision: str = "f32"):
-    """L = ||I(ne) - target||^2 and dL/dne (same dtype as ne)."""
+                    spacing, lwl: float, precision: str = "f32", group=None):
+    """L = ||I(ne) - target||^2 and dL/dne (same dtype as ne); with a process
+    group, over the rays of all its ranks (the same L and dL/dne on each)."""
     x = ne.detach().requires_grad_(True)
-    img = detector_image(x, rays, spec, origin=origin, spacing=spacing, lwl=lwl, precision=precision)
+    img = detector_image(x, rays, spec, origin=origin, spacing=spacing, lwl=lwl, precision=precision,
+                         group=group)
     loss = (img.to(torch.float64) - target.to(torch.float64)).pow(2).sum()
     loss.backward()
     return float(loss.detach()), x.grad

@@ -193,3 +193,32 @@ def test_gradient_against_finite_differences_128cube_1e6_rays():
     assert np.abs(a32 - fd).max() <= 1e-2 * scale, np.abs(a32 - fd).max() / scale
     # the whole FP32 gradient against the FP64 one
     assert float((g32.double() - g64).norm() / g64.norm()) < 1e-2
+
+
+def test_process_group_of_one_matches_the_local_model():
+    """With a process group (NCCL, here one rank) the image and the gradient
+    pass through an all-reduce each; over one rank they must equal the local
+    model's, up to the order of the splat and gradient atomics."""
+    import datetime
+    import socket
+
+    import torch.distributed as dist
+    h, ne0, ne1, rays, spec = _small()
+    target = _kernel(ne1, rays, h, spec, "f64")[0]
+    img, grad = _kernel(ne0, rays, h, spec, "f64", target)
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60), device_id=torch.device("cuda", 0))
+    try:
+        x = ne0.to("cuda").requires_grad_(True)
+        img_g = adjoint.detector_image(x, rays.to("cuda"), spec, origin=(-L / 2,) * 3, spacing=(h,) * 3, omega=OM,
+                                       precision="f64", group=dist.group.WORLD)
+        (img_g.double() - target.to("cuda")).pow(2).sum().backward()
+        torch.cuda.synchronize()
+        assert _rel(img_g.detach().cpu(), img) < 1e-12
+        assert _rel(x.grad.cpu(), grad) < 1e-12
+    finally:
+        dist.destroy_process_group()
