@@ -42,8 +42,9 @@ class RayServer:
     """Continuous-batching ray-trace server on one GPU.
 
     budget_bytes: HBM admission budget (the arena is allocated up front).
-    tiles_per_step: 1024-ray tiles per iteration (default: two per resident
-    tracer CTA). quantum: tiles per job per round-robin round.
+    tiles_per_step: 1024-ray tiles per iteration (default: four per resident
+    tracer CTA, 8 per SM; shorter iterations pay their launch and retire
+    overhead too often). quantum: tiles per job per round-robin round.
     """
 
     def __init__(self, budget_bytes: int, *, max_jobs: int = 256, tiles_per_step: Optional[int] = None,
@@ -54,7 +55,7 @@ class RayServer:
         cfg = capi.SlothServerConfig()
         cfg.budget_bytes = int(budget_bytes)
         cfg.max_jobs = int(max_jobs)
-        cfg.tiles_per_step = int(tiles_per_step or 4 * sms)
+        cfg.tiles_per_step = int(tiles_per_step or 8 * sms)
         cfg.quantum = int(quantum)
         cfg.reserved = 0
         h = ctypes.c_void_p()
