@@ -47,11 +47,15 @@ typedef struct {
     double k;
 } Samp;
 
-static void sample(const OracleParams* p, const double r[3], Samp* s) {
+/* clip != 0 clamps the point into the grid in cell units first: a clamp in
+ * metres can map back to a cell coordinate just above n - 1 by rounding, and
+ * then sample the fill value instead of the field's limit from inside. */
+static void sample(const OracleParams* p, const double r[3], int clip, Samp* s) {
     double u[3], t[3];
     int i[3];
     for (int a = 0; a < 3; ++a) {
         u[a] = (r[a] - p->origin[a]) / p->spacing[a];
+        if (clip) u[a] = u[a] < 0.0 ? 0.0 : (u[a] > (double)(p->n[a] - 1) ? (double)(p->n[a] - 1) : u[a]);
         if (!(u[a] >= 0.0 && u[a] <= (double)(p->n[a] - 1))) {
             memset(s, 0, sizeof(*s));
             return;
@@ -88,15 +92,9 @@ static double phase_rate(double ne, double omega) {
     return -omega * x / (1.0 + sqrt(om));
 }
 
-static void rhs(const OracleParams* p, const double r_in[3], int clip, double a[3], double* g, double* k) {
+static void rhs(const OracleParams* p, const double r[3], int clip, double a[3], double* g, double* k) {
     Samp s;
-    double r[3] = {r_in[0], r_in[1], r_in[2]};
-    if (clip)   /* a step cut at a face samples the field's limit from inside */
-        for (int d = 0; d < 3; ++d) {
-            const double lo = p->origin[d], hi = p->origin[d] + p->spacing[d] * (double)(p->n[d] - 1);
-            r[d] = r[d] < lo ? lo : (r[d] > hi ? hi : r[d]);
-        }
-    sample(p, r, &s);
+    sample(p, r, clip, &s);   /* a step cut at a face samples the field's limit from inside */
     a[0] = s.f[1];
     a[1] = s.f[2];
     a[2] = s.f[3];

@@ -228,9 +228,15 @@ class Grid:
         self.kappa = None if Te is None else kappa_inv_brems(self.ne, Te, Z, omega)
         self.nm1 = n_refrac(self.ne, omega) - 1.0
 
-    def sample(self, r, *, with_kappa=False, with_nm1=False):
-        """Interpolate the four fields (and kappa / n-1) at r (3, N); 0 outside."""
+    def sample(self, r, *, with_kappa=False, with_nm1=False, clip=None):
+        """Interpolate the four fields (and kappa / n-1) at r (3, N); 0 outside.
+        Points where `clip` (bool (N,)) is set are first clamped into the grid
+        in cell units: a clamp in metres can map back to a cell coordinate just
+        above n - 1 by rounding, and then sample the fill value instead of the
+        field's limit from inside."""
         u = [(r[a] - self.origin[a]) / self.spacing[a] for a in range(3)]
+        if clip is not None:
+            u = [np.where(clip, np.clip(u[a], 0.0, self.n[a] - 1), u[a]) for a in range(3)]
         oob = np.zeros(r.shape[1], dtype=bool)
         idx, t = [], []
         for a in range(3):
@@ -307,11 +313,8 @@ def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=
     hi = grid.origin + grid.spacing * (np.asarray(grid.n) - 1)
 
     def rhs(rr, clip=None):
-        if clip is not None and clip.any():
-            rr = rr.copy()
-            for a in range(3):
-                rr[a] = np.where(clip, np.clip(rr[a], lo[a], hi[a]), rr[a])
-        f, k, m = grid.sample(rr, with_kappa=inv_brems, with_nm1=(phase_mode == "reference"))
+        f, k, m = grid.sample(rr, with_kappa=inv_brems, with_nm1=(phase_mode == "reference"),
+                              clip=clip if clip is not None and clip.any() else None)
         a = f[:, 1:].T
         if phase_mode == "reference":
             g = grid.omega * m
