@@ -5,7 +5,9 @@ C ABI, against the oracle:
   configuration);
 * the 256^3 parabolic trough with rays of its 1000 x 1000 jittered launch
   lattice. The grid is the configuration's; the rays are every 50th lattice
-  ray, so that the FP64 oracle finishes in seconds.
+  ray, so that the FP64 oracle finishes in seconds;
+* a 128^3 Kolmogorov box with inverse bremsstrahlung, the headline mode at
+  a size the oracle can follow.
 
 The trough also has an analytic answer: its transverse motion is simple
 harmonic, x(t) = x0 cos(W t) + (vx0 / W) sin(W t) with W = c sqrt(n0/nc) / Lp,
@@ -77,3 +79,27 @@ def test_config_trough_256_lattice(precision):
     assert inner.sum() > 10_000
     dx = np.abs(k["state"][-1][0].astype(np.float64) - x_an)[inner].max() / L
     assert dx < (1e-9 if precision == "f64" else 1e-6), dx
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_kolmogorov_128_with_absorption(precision):
+    """The headline mode at a size where interior runs are long: a 128^3
+    Kolmogorov box (20% RMS), inverse bremsstrahlung at Te = 20 eV, Z = 1,
+    2e4 rays of a 3 mm beam, three saves; against the oracle."""
+    n = 128
+    h = L / (n - 1)
+    ne = workloads.kolmogorov_box(n, L=L, mean=1e25, rms=0.2, seed=31).numpy()
+    rays = workloads.gaussian_beam(20_000, waist=1.5e-3, L=L, seed=32).numpy()
+    sched = runtime.schedule_times(np.linspace(0.0, L, 3), (h, h, h))
+    kw = dict(project=True, plane=L / 2, inv_brems=True, Te=20.0, Z=1.0)
+    k = run_kernel(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched, precision=precision, **kw)
+    o = run_oracle(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched, **kw)
+    assert position_error(k["state"], o["state"], L) < _tol(precision)
+    assert direction_error(k["state"], o["state"]) < _tol(precision)
+    side = (np.abs(o["state"][-1][0]) > L / 2) | (np.abs(o["state"][-1][1]) > L / 2)
+    ph = np.abs(o["phase"]).max()
+    dph = np.abs(k["phase"] - o["phase"])
+    assert dph[:, ~side].max() <= _tol(precision) * ph
+    damp = np.abs(k["amp"].astype(np.float64) - o["amp"])
+    assert damp[:, ~side].max() < (1e-12 if precision == "f64" else 1e-6)
+    assert (k["steps"] != o["steps"]).mean() < 1e-3
