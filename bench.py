@@ -77,12 +77,15 @@ def committed_traffic(args):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms, written to
+    clocks_rank<i>.csv in $SLOTH_CLOCKS_DIR (default: the temp directory)."""
 
     def __init__(self, index):
+        import tempfile
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        folder = os.environ.get("SLOTH_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(folder, f"clocks_rank{index}.csv")
 
     def __enter__(self):
         try:
