@@ -28,7 +28,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "ray-steps/s, 512³ turb box 1e7 rays, ≤1e-6 rel err vs all-FP64 kernel; p99 latency"
 UNIT = "ray-steps/s"
-BYTES_PER_RAY_STEP = 512          # 4 RK4 stages x 8 corners x 16-byte float4 voxels
+BYTES_PER_RAY_STEP = 384          # 3 stages (4th-order Runge-Kutta-Nystrom) x 8 corners x 16-byte float4 voxels
 L = 5e-3
 LWL = 532e-9
 TE, ZION = 20.0, 1.0
@@ -204,7 +204,8 @@ def run_reference(args):
         "config": {"workload": f"{n}^3 Kolmogorov turbulent box (mean 1e19 cm^-3, 20% RMS), 1e7-ray 3 mm "
                                f"Gaussian beam, 532 nm, Te=20 eV, Z=1; each step a {per_step}-ray sample",
                    "note": "the reference (JAX/diffrax) cannot be installed on this image; its CPU path is "
-                           "stood in for by the oracle's FP64 C restatement (fixed-step RK4)"},
+                           "stood in for by the oracle's FP64 C restatement (fixed-step 4th-order "
+                           "Runge-Kutta-Nystrom, the tracers' method)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port",
                          "sample": f"{per_step} rays per step, {args.steps} steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -536,7 +537,7 @@ def run_sloth(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{n}^3 Kolmogorov turbulent box (mean 1e19 cm^-3, 20% RMS, k^-11/3), "
                                    f"{nrays:.0e} rays, 3 mm Gaussian beam along +z, 532 nm, Te=20 eV, Z=1, "
-                                   "fixed-step RK4 ds=h/2, detector plane z=+2.5 mm",
+                                   "fixed-step 4th-order Runge-Kutta-Nystrom ds=h/2, detector plane z=+2.5 mm",
                        "l2": f"inputs larger than L2 ({n ** 3 * 16 / 1e9:.2f} GB packed grid, "
                              f"{nrays * 24 / 1e6:.0f} MB rays)",
                        "precision": "FP32 state with compensated sums, FP64 phase, Kahan FP32 optical depth",
@@ -550,7 +551,7 @@ def run_sloth(args):
                          "bytes_per_ray_step": BYTES_PER_RAY_STEP,
                          "dram_achieved": (traffic / (kms / 1e3) / 1e9) if traffic else None,
                          "dram_frac": (traffic / (kms / 1e3) / 1e9 / peak) if traffic else None,
-                         "note": "achieved = logical gather bytes (4 RK4 stages x 8 corners x 16 B per ray-step); "
+                         "note": "achieved = logical gather bytes (3 stages x 8 corners x 16 B per ray-step); "
                                  "the corners come from a register cell cache and L1, so physical DRAM traffic "
                                  "(traffic, dram_frac, from ncu) is ~1.5 B per ray-step; the kernel is bound by "
                                  "its FP32 pipes: instruction issue at ~59% of peak, FMA pipe ~66% active "

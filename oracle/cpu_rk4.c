@@ -1,5 +1,6 @@
 /*
- * cpu_rk4.c -- FP64 CPU restatement of SLOTH's ray trace with fixed-step RK4.
+ * cpu_rk4.c -- FP64 CPU restatement of SLOTH's ray trace with a fixed-step
+ * fourth-order Runge-Kutta(-Nystrom) integrator, the method of the CUDA tracers.
  *
  * TEST INFRASTRUCTURE ONLY: the checker for the CUDA tracers and the timed
  * CPU baseline. Nothing in the product links or calls it.
@@ -145,32 +146,25 @@ static int inside(const OracleParams* p, const double r[3]) {
     return 1;
 }
 
-/* One RK4 step of length h (seconds) of r' = v, v' = grad G, phase, tau. */
-static void rk4(const OracleParams* p, double h, int clip, double r[3], double v[3], double* ph, double* ta) {
-    double a1[3], a2[3], a3[3], a4[3], r2[3], v2[3], r3[3], v3[3], r4[3], v4[3];
-    double g1, g2, g3, g4, k1, k2, k3, k4;
+/* One step of length h (seconds) of r'' = grad G(r) with phase' = g(r) and
+ * tau' = kappa(r): Nystrom's fourth-order Runge-Kutta-Nystrom method (three
+ * samples), with Simpson's weights for the two integrals:
+ *   r2 = r + h/2 v + h^2/8 a1,  r3 = r + h v + h^2/2 a2,
+ *   r' = r + h v + h^2/6 (a1 + 2 a2),  v' = v + h/6 (a1 + 4 a2 + a3). */
+static void step_rkn(const OracleParams* p, double h, int clip, double r[3], double v[3], double* ph, double* ta) {
+    double a1[3], a2[3], a3[3], r2[3], r3[3];
+    double g1, g2, g3, k1, k2, k3;
     rhs(p, r, clip, a1, &g1, &k1);
-    for (int a = 0; a < 3; ++a) {
-        r2[a] = r[a] + 0.5 * h * v[a];
-        v2[a] = v[a] + 0.5 * h * a1[a];
-    }
+    for (int a = 0; a < 3; ++a) r2[a] = r[a] + 0.5 * h * v[a] + (h * h / 8.0) * a1[a];
     rhs(p, r2, clip, a2, &g2, &k2);
-    for (int a = 0; a < 3; ++a) {
-        r3[a] = r[a] + 0.5 * h * v2[a];
-        v3[a] = v[a] + 0.5 * h * a2[a];
-    }
+    for (int a = 0; a < 3; ++a) r3[a] = r[a] + h * v[a] + (h * h / 2.0) * a2[a];
     rhs(p, r3, clip, a3, &g3, &k3);
     for (int a = 0; a < 3; ++a) {
-        r4[a] = r[a] + h * v3[a];
-        v4[a] = v[a] + h * a3[a];
+        r[a] = r[a] + h * v[a] + (h * h / 6.0) * (a1[a] + 2.0 * a2[a]);
+        v[a] = v[a] + h / 6.0 * (a1[a] + 4.0 * a2[a] + a3[a]);
     }
-    rhs(p, r4, clip, a4, &g4, &k4);
-    for (int a = 0; a < 3; ++a) {
-        r[a] += h / 6.0 * (v[a] + 2.0 * v2[a] + 2.0 * v3[a] + v4[a]);
-        v[a] += h / 6.0 * (a1[a] + 2.0 * a2[a] + 2.0 * a3[a] + a4[a]);
-    }
-    *ph += h / 6.0 * (g1 + 2.0 * g2 + 2.0 * g3 + g4);
-    *ta += h / 6.0 * (k1 + 2.0 * k2 + 2.0 * k3 + k4);
+    *ph += h / 6.0 * (g1 + 4.0 * g2 + g3);
+    *ta += h / 6.0 * (k1 + 4.0 * k2 + k3);
 }
 
 /* A ray inside the grid whose straight-line prediction leaves it within the
@@ -234,7 +228,7 @@ static long long trace_one(const OracleParams* p, const double* rays, int64_t n,
             }
             const int split = phi < 1.0;
             if (phi < 0.0) phi = 0.0;
-            rk4(p, dt * phi, split || near, r, v, &ph, &ta);
+            step_rkn(p, dt * phi, split || near, r, v, &ph, &ta);
             ++nst;
             if (split) frozen_t = (double)step + phi;
         }

@@ -14,7 +14,8 @@ Every function restates the reference (paths relative to the SLOTH repo):
 * ``dndr``, ``dsdt``                     src/core/propagator.py:96-114, :168-243
 * ``ray_to_Jonesvector``, ``back_propogate``  src/shared/propagation.py:4-134
 * phase integrand omega*(n - 1)          src/legacy/full_solver.py:271-274, :341-347
-* ``trace_rays``: the fixed-step RK4 integration of dsdt (+ phase) that
+* ``trace_rays``: the fixed-step fourth-order Runge-Kutta-Nystrom
+  integration of dsdt (+ phase) that
   replaces diffrax's adaptive Tsit5 (src/core/propagator.py:731-793) in this
   build, with the reference's time normalisation and save semantics
   (:616-617, :1133-1138) and keep_current_plane projection (:316-327).
@@ -276,12 +277,16 @@ def phase_integrand(ne_interp, omega, nc):
 def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=2,
                project=False, plane=0.0, inv_brems=False, early_exit=True,
                phase_mode="kernel"):
-    """Fixed-step RK4 of dsdt (+ phase, + optical depth) in SI units.
+    """Fixed-step fourth-order Runge-Kutta-Nystrom integration of dsdt
+    (+ phase, + optical depth) in SI units: three samples per step,
+    r2 = r + h/2 v + h^2/8 a1, r3 = r + h v + h^2/2 a2, r' = r + h v +
+    h^2/6 (a1 + 2 a2), v' = v + h/6 (a1 + 4 a2 + a3), Simpson's weights for
+    the phase and the depth.
 
     Step dt = dtau/c. Save j after step first_save + j*save_every. The RHS is
     discontinuous at the grid faces (gradients inside, fill 0 outside), so a
     step of a ray inside the grid whose straight-line prediction r + v*dt
-    leaves the grid is shortened to end on the face (an RK4 step of dt*phi,
+    leaves the grid is shortened to end on the face (a step of dt*phi,
     phi = the smallest positive (face - r)/(v*dt)); the ray is then frozen and
     advanced to later saves by straight-line drift from its exit time. A ray
     outside the grid on an axis and moving away on it is frozen likewise.
@@ -378,17 +383,17 @@ def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=
             clamp = split | near
             phi = np.maximum(phi, 0.0)
             h = dt * phi
+            # Nystrom's fourth-order Runge-Kutta-Nystrom step (r'' = a(r);
+            # three samples), Simpson's weights for the phase and the depth
             a1, g1, k1 = rhs(rr, clamp)
-            r2, v2 = rr + 0.5 * h * vv, vv + 0.5 * h * a1
+            r2 = rr + 0.5 * h * vv + (h * h / 8.0) * a1
             a2, g2, k2 = rhs(r2, clamp)
-            r3, v3 = rr + 0.5 * h * v2, vv + 0.5 * h * a2
+            r3 = rr + h * vv + (h * h / 2.0) * a2
             a3, g3, k3 = rhs(r3, clamp)
-            r4, v4 = rr + h * v3, vv + h * a3
-            a4, g4, k4 = rhs(r4, clamp)
-            r[:, idx] = rr + h / 6.0 * (vv + 2 * v2 + 2 * v3 + v4)
-            v[:, idx] = vv + h / 6.0 * (a1 + 2 * a2 + 2 * a3 + a4)
-            phase[idx] += h / 6.0 * (g1 + 2 * g2 + 2 * g3 + g4)
-            tau[idx] += h / 6.0 * (k1 + 2 * k2 + 2 * k3 + k4)
+            r[:, idx] = rr + h * vv + (h * h / 6.0) * (a1 + 2 * a2)
+            v[:, idx] = vv + h / 6.0 * (a1 + 4 * a2 + a3)
+            phase[idx] += h / 6.0 * (g1 + 4 * g2 + g3)
+            tau[idx] += h / 6.0 * (k1 + 4 * k2 + k3)
             steps[idx] += 1
             if split.any():
                 sidx = idx[split]

@@ -6,7 +6,7 @@
 // double2 (32 bytes per voxel).
 //
 // Ray coordinates inside the tracers are in grid cells (p = (x - x0)/h) and
-// the velocity in cells per step (w = (v/c) * dtau / h), so one RK4 step is a
+// the velocity in cells per step (w = (v/c) * dtau / h), so one integration step is a
 // unit step and dw/dstep = S * dq/du with S = -(dtau/h)^2 / 2.
 #pragma once
 

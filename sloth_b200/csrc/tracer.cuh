@@ -1,5 +1,5 @@
 // Device code shared by the tracer entry points (trace.cu) and the request
-// server (server.cu): kernel arguments, samplers, the RK4 step, per-ray
+// server (server.cu): kernel arguments, samplers, the integration step, per-ray
 // bookkeeping, the per-tile tracing loop and the Morton pre-pass.
 //
 // What the reference does (src/core/propagator.py):
@@ -9,15 +9,16 @@
 //   solve / trace_and_save_depths (:723-793, :1159-1198): vmap of a diffrax
 //                    solve from t = 0 to the save times; output through
 //                    ray_to_Jonesvector (src/shared/propagation.py:4-90).
-// What runs here: the same ODE with fixed-step RK4 in scaled units (grid
-// cells, cells per step), one thread per ray, plus the optical phase integral
-// of omega*(n - 1) (src/legacy/full_solver.py:341-347, n = sqrt(1 - ne/nc))
-// and the inverse-bremsstrahlung optical depth, both as RK4 quadratures of
-// the stage values, and the Jones-vector projection at each save.
+// What runs here: the same ODE with a fixed-step fourth-order Runge-Kutta-
+// Nystrom method in scaled units (grid cells, cells per step; see rkn_step),
+// one thread per ray, plus the optical phase integral of omega*(n - 1)
+// (src/legacy/full_solver.py:341-347, n = sqrt(1 - ne/nc)) and the
+// inverse-bremsstrahlung optical depth, both as Simpson quadratures of the
+// stage values, and the Jones-vector projection at each save.
 //
 // Grid faces: the RHS jumps to the outside fill there. A step whose
-// straight-line prediction p + w crosses a face is cut to end on it (RK4 with
-// a fraction phi of the step) and the ray then leaves on a straight line; a
+// straight-line prediction p + w crosses a face is cut to end on it (a step
+// of a fraction phi) and the ray then leaves on a straight line; a
 // step whose prediction ends within kFaceMargin cells of a face, or is cut,
 // samples its stage points clamped into the grid, i.e. it integrates the
 // field's limit from inside, so that no stage sits on the discontinuity.
@@ -69,10 +70,10 @@ enum { SAMPLE_PLAIN = 0, SAMPLE_CLAMP = 1, SAMPLE_INTERIOR = 2 };
 
 // Largest |acceleration| (cells per step^2) for which an interior step
 // (ray inside, prediction p + w at least kFaceMargin inside on every axis)
-// has every stage point inside: the stages sit at p + w/2 + A1/4 and
+// has every stage point inside: the stages sit at p + w/2 + A1/8 and
 // p + w + A2/2, at least kFaceMargin/2 and kFaceMargin from the faces before
-// the A terms, so |A| <= 4 * (kFaceMargin/2) = 0.04 suffices; 0.03 keeps
-// headroom for rounding.
+// the A terms, so |A| <= min(8 * kFaceMargin/2, 2 * kFaceMargin) = 0.04
+// suffices; 0.03 keeps headroom for rounding.
 constexpr double kInteriorAccel = 0.03;
 
 // ---------------------------------------------------------------------------
@@ -181,11 +182,15 @@ __device__ __forceinline__ void poly_coeffs(R (&t)[8], R v0, R v1, R v2, R v3, R
     t[7] = ((v7 - v6) - dxz) - (dyz - bz); // cxyz
 }
 
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 template <class R>
 __device__ __forceinline__ R poly_eval(const R (&t)[8], R fx, R fy, R fz) {
-    const R cz = (t[3] + fx * t[5]) + fy * (t[6] + fx * t[7]);   // coefficient of fz
-    const R cy = t[2] + fx * t[4];                               // coefficient of fy (without fz)
-    return ((t[0] + fx * t[1]) + fy * cy) + fz * cz;
+    // explicit fused multiply-adds: every kernel that inlines this rounds alike
+    const R cz = fma_rn(fy, fma_rn(fx, t[7], t[6]), fma_rn(fx, t[5], t[3]));   // coefficient of fz
+    const R cy = fma_rn(fx, t[4], t[2]);                                         // of fy (without fz)
+    return fma_rn(fz, cz, fma_rn(fy, cy, fma_rn(fx, t[1], t[0])));
 }
 
 // FP32 cell cache on paired instructions. The packed voxel is a float4
@@ -263,6 +268,15 @@ __device__ __forceinline__ float2 nm1_series2(float2 x) {
     t = __ffma2_rn(x, t, make_float2(0.125f, 0.125f));
     t = __ffma2_rn(x, t, make_float2(0.5f, 0.5f));
     return __fmul2_rn(make_float2(-x.x, -x.y), t);
+}
+
+// The same series for one argument, rounded exactly as each lane of the pair.
+__device__ __forceinline__ float nm1_series1(float x) {
+    float t = __fmaf_rn(x, 0.02734375f, 0.0390625f);
+    t = __fmaf_rn(x, t, 0.0625f);
+    t = __fmaf_rn(x, t, 0.125f);
+    t = __fmaf_rn(x, t, 0.5f);
+    return __fmul_rn(-x, t);
 }
 
 // Inverse-bremsstrahlung rate of one grid point per kappa_q2: q^2 * CL(q),
@@ -472,22 +486,29 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
     }
 }
 
-// One RK4 step of length phi (in steps; phi = 1 except for a step cut at a
-// grid face) in scaled units; see the file header. Stage sums are
-// accumulated as the stages are produced to keep few values live:
-//   p' = p + phi*w + phi^2 (A1 + A2 + A3)/6,  w' = w + phi (A1 + 2A2 + 2A3 + A4)/6,
-//   stage points p, p + phi*w/2, p + phi*w2/2, p + phi*w3
-//   with w2 = w + phi*A1/2, w3 = w + phi*A2/2.
+// One step of length phi (in steps; phi = 1 except for a step cut at a grid
+// face) in scaled units; see the file header. The ray equation is second
+// order with a position-only force, p'' = A(p), and the phase and optical
+// depth integrate functions of the position only, so the step is Nystrom's
+// fourth-order Runge-Kutta-Nystrom method, three samples of the field instead
+// of RK4's four:
+//   stage points p, p + phi*w/2 + phi^2 A1/8, p + phi*w + phi^2 A2/2,
+//   p' = p + phi*w + phi^2 (A1 + 2 A2)/6,  w' = w + phi (A1 + 4 A2 + A3)/6,
+// and the phase and depth take Simpson's weights (1, 4, 1)/6 on the stages.
+// The position and velocity are fourth order; the two integrals are third
+// order in the step (their middle stage point is second order), an error
+// many orders below the FP32 rounding here. Stage sums are accumulated as the
+// stages are produced to keep few values live.
 // The phase integrand is n - 1 with n = sqrt(1 - (omega_pe/omega)^2) from the
 // interpolated density (src/legacy/full_solver.py:271-274, :341-347).
 template <class P, int IB, bool SMALLX, int MODE, class Cache>
-__device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
+__device__ __forceinline__ void rkn_step(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
     using R = typename P::R;
-    const R two = R(2);
     const R hphi = R(0.5) * phi, phi6 = phi * R(1.0 / 6.0), phi2_6 = phi * phi6;
+    const R phi2_8 = R(0.125) * phi * phi, phi2_2 = R(0.5) * phi * phi;
     const R S0 = arg_S<R>(a, 0), S1 = arg_S<R>(a, 1), S2 = arg_S<R>(a, 2);
     const R ope2 = arg_ope2<R>(a);
-    R ph[3], pl[3], we[3], sA[3], sW[3], w3[3], st[3];
+    R ph[3], pl[3], we[3], sA[3], sW[3], st[3];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         ph[x] = r.p[x].hi();
@@ -495,12 +516,11 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
         we[x] = r.w[x].val();
     }
     Sample<P> s;
-    // stage 1 at p
-    // FP32 with the series form of n - 1 evaluates it for stages (1, 2) and
-    // (3, 4) as pairs
+    // FP32 with the series form of n - 1 evaluates it for stages 1 and 2 as a pair
     constexpr bool kPairPhase = SMALLX && sizeof(R) == 4;
+    // stage 1 at p
     sample_c<P, IB, MODE>(a, ph, pl, s, cc);
-    R g, q1 = R(0), q3 = R(0);
+    R g, q1 = R(0);
     if constexpr (kPairPhase) {
         q1 = s.q;
         g = R(0);
@@ -508,58 +528,37 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
         g = nm1<P, SMALLX>(ope2 * s.q);
     }
     R kq = s.k;
-    sA[0] = S0 * s.g0; sA[1] = S1 * s.g1; sA[2] = S2 * s.g2;
-    // stage 2 at p + phi*w/2
-#pragma unroll
-    for (int x = 0; x < 3; ++x) {
-        sW[x] = sA[x];
-        st[x] = pl[x] + hphi * we[x];
-    }
-    sample_c<P, IB, MODE>(a, ph, st, s, cc);
-#pragma unroll
-    for (int x = 0; x < 3; ++x) st[x] = pl[x] + hphi * (we[x] + hphi * sA[x]);   // p + phi*w2/2
     {
         const R A[3] = {S0 * s.g0, S1 * s.g1, S2 * s.g2};
 #pragma unroll
         for (int x = 0; x < 3; ++x) {
-            w3[x] = we[x] + hphi * A[x];
-            sA[x] += A[x];
-            sW[x] += two * A[x];
+            sA[x] = A[x];
+            sW[x] = A[x];
+            st[x] = pl[x] + (hphi * we[x] + phi2_8 * A[x]);     // p + phi*w/2 + phi^2 A1/8
+        }
+    }
+    // stage 2
+    sample_c<P, IB, MODE>(a, ph, st, s, cc);
+    {
+        const R A[3] = {S0 * s.g0, S1 * s.g1, S2 * s.g2};
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            sA[x] += R(2) * A[x];
+            sW[x] += R(4) * A[x];
+            st[x] = pl[x] + (phi * we[x] + phi2_2 * A[x]);      // p + phi*w + phi^2 A2/2
         }
     }
     if constexpr (kPairPhase) {
         const float2 n12 = nm1_series2(__fmul2_rn(make_float2(ope2, ope2), make_float2(q1, s.q)));
-        g = n12.x + two * n12.y;
+        g = n12.x + R(4) * n12.y;
     } else {
-        g += two * nm1<P, SMALLX>(ope2 * s.q);
+        g += R(4) * nm1<P, SMALLX>(ope2 * s.q);
     }
-    kq += two * s.k;
-    // stage 3 at p + phi*w2/2
-    sample_c<P, IB, MODE>(a, ph, st, s, cc);
-    {
-        const R A[3] = {S0 * s.g0, S1 * s.g1, S2 * s.g2};
-#pragma unroll
-        for (int x = 0; x < 3; ++x) {
-            sA[x] += A[x];
-            sW[x] += two * A[x];
-            st[x] = pl[x] + phi * w3[x];
-        }
-    }
-    if constexpr (kPairPhase) {
-        q3 = s.q;
-    } else {
-        g += two * nm1<P, SMALLX>(ope2 * s.q);
-    }
-    kq += two * s.k;
-    // stage 4 at p + phi*w3
+    kq += R(4) * s.k;
+    // stage 3
     sample_c<P, IB, MODE>(a, ph, st, s, cc);
     sW[0] += S0 * s.g0; sW[1] += S1 * s.g1; sW[2] += S2 * s.g2;
-    if constexpr (kPairPhase) {
-        const float2 n34 = nm1_series2(__fmul2_rn(make_float2(ope2, ope2), make_float2(q3, s.q)));
-        g += two * n34.x + n34.y;
-    } else {
-        g += nm1<P, SMALLX>(ope2 * s.q);
-    }
+    g += nm1<P, SMALLX>(ope2 * s.q);
     kq += s.k;
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
@@ -639,14 +638,22 @@ __device__ __forceinline__ void kahan2(float2& s, float2& c, float2 x) {
     s = t;
 }
 
-template <int IB, bool SMALLX, int MODE, int NK>
-__device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, CellPolyF2<NK>& cc, float phi) {
-    const float two = 2.0f;
+// UNIT: phi is 1 (every step but a cut one); the multiplications by phi are
+// left out, which gives bitwise the results of the general form at phi = 1
+// (fma(1, a, b) rounds as a + b).
+template <int IB, bool SMALLX, int MODE, bool UNIT, int NK>
+__device__ __forceinline__ void rkn_step_f2(const TraceArgs& a, Ray<PolF32>& r, CellPolyF2<NK>& cc, float phi) {
+    if constexpr (UNIT) phi = 1.0f;
+    auto mphi = [&](float x) { return UNIT ? x : __fmul_rn(phi, x); };
+    auto mphi2 = [&](float2 x) { return UNIT ? x : __fmul2_rn(bc2(phi), x); };
     const float hphi = 0.5f * phi, phi6 = phi * (1.0f / 6.0f), phi2_6 = phi * phi6;
+    const float phi2_8 = 0.125f * phi * phi, phi2_2 = 0.5f * phi * phi;
     const float S0 = a.Sf[0];
     const float2 S12 = make_float2(a.Sf[1], a.Sf[2]);
     const float ope2 = a.ope2f;
-    const float2 hphi2 = bc2(hphi), two2 = bc2(two);
+    const float2 hphi2 = bc2(hphi), phi22 = bc2(phi), phi2_82 = bc2(phi2_8), phi2_22 = bc2(phi2_2);
+    // Every rounding is explicit (intrinsics), so that each kernel that
+    // inlines this step (the tracer's and the server's) rounds alike.
     const float phx = r.p[0].s, plx = r.p[0].c, wex = r.w[0].s + r.w[0].c;
     const float2 phyz = make_float2(r.p[1].s, r.p[2].s), plyz = make_float2(r.p[1].c, r.p[2].c);
     const float2 weyz = __fadd2_rn(make_float2(r.w[1].s, r.w[2].s), make_float2(r.w[1].c, r.w[2].c));
@@ -654,71 +661,54 @@ __device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
     Sample<PolF32> s;
     // stage 1 at p
     sample_f2<IB, MODE>(a, phx, plx, phyz, plyz, s, cc);
-    float g = 0.0f, q1 = 0.0f, q3 = 0.0f;
-    if constexpr (kPairPhase) q1 = s.q; else g = nm1<PolF32, SMALLX>(ope2 * s.q);
+    float g = 0.0f, q1 = 0.0f;
+    if constexpr (kPairPhase) q1 = s.q; else g = nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q));
     float kq = s.k;
-    float sAx = S0 * s.g0;
+    float sAx = __fmul_rn(S0, s.g0);
     float2 sAyz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
     float sWx = sAx;
     float2 sWyz = sAyz;
-    // stage 2 at p + phi*w/2
-    float stx = plx + hphi * wex;
-    float2 styz = __ffma2_rn(hphi2, weyz, plyz);
+    // stage 2 at p + phi*w/2 + phi^2 A1/8
+    float stx = __fadd_rn(plx, __fmaf_rn(phi2_8, sAx, __fmul_rn(hphi, wex)));
+    float2 styz = __fadd2_rn(plyz, __ffma2_rn(phi2_82, sAyz, __fmul2_rn(hphi2, weyz)));
     sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
-    stx = plx + hphi * (wex + hphi * sAx);                        // p + phi*w2/2
-    styz = __ffma2_rn(hphi2, __ffma2_rn(hphi2, sAyz, weyz), plyz);
-    float w3x;
-    float2 w3yz;
     {
-        const float Ax = S0 * s.g0;
+        const float Ax = __fmul_rn(S0, s.g0);
         const float2 Ayz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
-        w3x = wex + hphi * Ax;
-        w3yz = __ffma2_rn(hphi2, Ayz, weyz);
-        sAx += Ax;
-        sAyz = __fadd2_rn(sAyz, Ayz);
-        sWx += two * Ax;
-        sWyz = __ffma2_rn(two2, Ayz, sWyz);
+        sAx = __fmaf_rn(2.0f, Ax, sAx);
+        sAyz = __ffma2_rn(bc2(2.0f), Ayz, sAyz);
+        sWx = __fmaf_rn(4.0f, Ax, sWx);
+        sWyz = __ffma2_rn(bc2(4.0f), Ayz, sWyz);
+        // stage 3 at p + phi*w + phi^2 A2/2
+        stx = __fadd_rn(plx, __fmaf_rn(phi2_2, Ax, mphi(wex)));
+        styz = __fadd2_rn(plyz, __ffma2_rn(phi2_22, Ayz, mphi2(weyz)));
     }
     if constexpr (kPairPhase) {
         const float2 n12 = nm1_series2(__fmul2_rn(bc2(ope2), make_float2(q1, s.q)));
-        g = n12.x + two * n12.y;
+        g = __fmaf_rn(4.0f, n12.y, n12.x);
     } else {
-        g += two * nm1<PolF32, SMALLX>(ope2 * s.q);
+        g = __fmaf_rn(4.0f, nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q)), g);
     }
-    kq += two * s.k;
-    // stage 3 at p + phi*w2/2
+    kq = __fmaf_rn(4.0f, s.k, kq);
     sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
-    {
-        const float Ax = S0 * s.g0;
-        const float2 Ayz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
-        sAx += Ax;
-        sAyz = __fadd2_rn(sAyz, Ayz);
-        sWx += two * Ax;
-        sWyz = __ffma2_rn(two2, Ayz, sWyz);
-        stx = plx + phi * w3x;
-        styz = __ffma2_rn(bc2(phi), w3yz, plyz);
-    }
-    if constexpr (kPairPhase) q3 = s.q; else g += two * nm1<PolF32, SMALLX>(ope2 * s.q);
-    kq += two * s.k;
-    // stage 4 at p + phi*w3
-    sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
-    sWx += S0 * s.g0;
+    sWx = __fmaf_rn(S0, s.g0, sWx);
     sWyz = __ffma2_rn(S12, make_float2(s.g1, s.g2), sWyz);
-    if constexpr (kPairPhase) {
-        const float2 n34 = nm1_series2(__fmul2_rn(bc2(ope2), make_float2(q3, s.q)));
-        g += two * n34.x + n34.y;
-    } else {
-        g += nm1<PolF32, SMALLX>(ope2 * s.q);
-    }
-    kq += s.k;
+    if constexpr (kPairPhase)
+        g = __fadd_rn(g, nm1_series1(__fmul_rn(ope2, s.q)));
+    else
+        g = __fadd_rn(g, nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q)));
+    kq = __fadd_rn(kq, s.k);
     // x: the scalar update
-    r.p[0].add(phi * r.w[0].hi() + (phi * r.w[0].lo() + phi2_6 * sAx));
-    r.w[0].add(phi6 * sWx);
+    if constexpr (UNIT)
+        r.p[0].add(__fadd_rn(r.w[0].hi(), __fadd_rn(r.w[0].lo(), __fmul_rn(phi2_6, sAx))));
+    else
+        r.p[0].add(__fmaf_rn(phi, r.w[0].hi(), __fmaf_rn(phi, r.w[0].lo(), __fmul_rn(phi2_6, sAx))));
+    r.w[0].add(__fmul_rn(phi6, sWx));
     // y, z: the same update on pairs
     {
-        const float2 phi2 = bc2(phi);
         const float2 whi = make_float2(r.w[1].s, r.w[2].s), wlo = make_float2(r.w[1].c, r.w[2].c);
-        const float2 dp = __ffma2_rn(phi2, whi, __ffma2_rn(phi2, wlo, __fmul2_rn(bc2(phi2_6), sAyz)));
+        const float2 dp = UNIT ? __fadd2_rn(whi, __fadd2_rn(wlo, __fmul2_rn(bc2(phi2_6), sAyz)))
+                               : __ffma2_rn(phi22, whi, __ffma2_rn(phi22, wlo, __fmul2_rn(bc2(phi2_6), sAyz)));
         float2 ps = phyz, pc = plyz;
         kahan2(ps, pc, dp);
         r.p[1].s = ps.x; r.p[2].s = ps.y; r.p[1].c = pc.x; r.p[2].c = pc.y;
@@ -726,18 +716,18 @@ __device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
         kahan2(ws, wc, __fmul2_rn(bc2(phi6), sWyz));
         r.w[1].s = ws.x; r.w[2].s = ws.y; r.w[1].c = wc.x; r.w[2].c = wc.y;
     }
-    r.ph += (double)(phi * g);
-    if constexpr (IB != IB_OFF) r.tau.add(phi * kq);
+    r.ph += (double)mphi(g);
+    if constexpr (IB != IB_OFF) r.tau.add(mphi(kq));
 }
 
-// One RK4 step: the paired FP32 form with the paired cell cache, the generic
-// form otherwise.
-template <class P, int IB, bool SMALLX, int MODE, class Cache>
+// One step: the paired FP32 form with the paired cell cache, the generic form
+// otherwise.
+template <class P, int IB, bool SMALLX, int MODE, bool UNIT = false, class Cache>
 __device__ __forceinline__ void step_any(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
     if constexpr (IsPairedCache<Cache>::value && SLOTH_PAIRED_STEP) {
-        rk4_step_f2<IB, SMALLX, MODE>(a, r, cc, phi);
+        rkn_step_f2<IB, SMALLX, MODE, UNIT>(a, r, cc, phi);
     } else {
-        rk4_step<P, IB, SMALLX, MODE>(a, r, cc, phi);
+        rkn_step<P, IB, SMALLX, MODE>(a, r, cc, phi);
     }
 }
 
@@ -1051,13 +1041,13 @@ __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, 
             if (FAST && kind == 0) {
 #pragma unroll 1
                 for (int e = 0;; ++e) {
-                    step_any<P, IB, SMALLX, SAMPLE_INTERIOR>(a, r, cc, typename P::R(1));
+                    step_any<P, IB, SMALLX, SAMPLE_INTERIOR, true>(a, r, cc, typename P::R(1));
                     if (e == extra) break;
                     ++r.step;
                 }
                 r.run -= extra;
             } else if (kind == 0 || kind == 3) {
-                step_any<P, IB, SMALLX, SAMPLE_PLAIN>(a, r, cc, typename P::R(1));
+                step_any<P, IB, SMALLX, SAMPLE_PLAIN, true>(a, r, cc, typename P::R(1));
             } else {
                 step_any<P, IB, SMALLX, SAMPLE_CLAMP>(a, r, cc, phi);
                 if (kind == 2) {

@@ -1,26 +1,26 @@
 """The tracer skips its per-step face test for runs of steps it has proven to
 be interior steps. The proof: with every stage acceleration bounded by B
-(cells per step^2), after j RK4 unit steps from (p, w)
+(cells per step^2), after j unit steps from (p, w)
 
     |w_j - w| <= j B,   |p_j - p - j w| <= B j^2 / 2,
 
 so the position p_j and the prediction p_j + w_j lie within B (j^2/2 + j) of
 the segment from p + w to p + (j + 1) w. This checks the envelope against
-RK4 steps driven by adversarial accelerations (every stage at +-B, chosen at
+the tracer's steps driven by adversarial accelerations (every stage at +-B, chosen at
 random or to push one way), in FP64 on the CPU."""
 import numpy as np
 import pytest
 
 
-def _rk4_step(p, w, accel):
-    """The tracer's unit RK4 step (phi = 1): stages at p, p + w/2,
-    p + w/2 + A1/4, p + w + A2/2; p' = p + w + (A1 + A2 + A3)/6,
-    w' = w + (A1 + 2 A2 + 2 A3 + A4)/6. `accel` gives each stage's A."""
+def _rkn_step(p, w, accel):
+    """The tracer's unit step (phi = 1), Nystrom's fourth-order
+    Runge-Kutta-Nystrom method: stages at p, p + w/2 + A1/8, p + w + A2/2;
+    p' = p + w + (A1 + 2 A2)/6, w' = w + (A1 + 4 A2 + A3)/6. `accel` gives
+    each stage's A."""
     a1 = accel(p)
-    a2 = accel(p + w / 2)
-    a3 = accel(p + w / 2 + a1 / 4)
-    a4 = accel(p + w + a2 / 2)
-    return p + w + (a1 + a2 + a3) / 6, w + (a1 + 2 * a2 + 2 * a3 + a4) / 6
+    a2 = accel(p + w / 2 + a1 / 8)
+    a3 = accel(p + w + a2 / 2)
+    return p + w + (a1 + 2 * a2) / 6, w + (a1 + 4 * a2 + a3) / 6
 
 
 @pytest.mark.parametrize("mode", ["random", "push", "alternate"])
@@ -44,7 +44,7 @@ def test_run_envelope_holds(mode, m):
 
         p, w = p0.copy(), w0.copy()
         for j in range(1, m + 1):
-            p, w = _rk4_step(p, w, accel)
+            p, w = _rkn_step(p, w, accel)
             dev = B * (j * j / 2 + j)
             assert np.all(np.abs(w - w0) <= j * B * (1 + 1e-12))
             assert np.all(np.abs(p - p0 - j * w0) <= B * j * j / 2 * (1 + 1e-12) + 1e-12)
@@ -60,5 +60,5 @@ def test_push_reaches_the_position_bound():
     B, m = 0.03, 31
     p, w = np.zeros(3), np.zeros(3)
     for _ in range(m):
-        p, w = _rk4_step(p, w, lambda _x: np.full(3, B))
+        p, w = _rkn_step(p, w, lambda _x: np.full(3, B))
     assert np.allclose(p, B * m * m / 2) and np.allclose(w, B * m)
