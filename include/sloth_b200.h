@@ -57,7 +57,8 @@ typedef struct SlothGridDesc {
     double  spacing[3];  /* uniform spacing per axis (m), > 0                 */
 } SlothGridDesc;
 
-/* Fixed-step RK4 schedule and physics of one trace.
+/* Fixed-step schedule and physics of one trace (fourth-order Runge-Kutta-
+ * Nystrom steps: three field samples per step).
  * All steps have the same length dtau (tau = c*t, metres). Save j (0-based)
  * is taken after step first_save + j*save_every; the trace ends at the last
  * save. Rays that have left the grid for good are advanced to later saves by
@@ -106,7 +107,7 @@ typedef struct SlothTraceOutputs {
                                integral of omega*(n-1) dt (rad)                     */
     void*     amp;          /* [S][N] optional: exp(-tau_ib); needs inv_brems       */
     uint8_t*  status;       /* [N] optional: SLOTH_RAY_*                            */
-    int32_t*  steps;        /* [N] optional: RK4 steps taken before exit / end      */
+    int32_t*  steps;        /* [N] optional: steps taken before exit / end          */
     unsigned long long* total_steps; /* [1] optional device counter: sum of steps,
                                zeroed by the entry point before the launch          */
     void*     trace_event_begin; /* optional cudaEvent_t recorded on `stream` right

@@ -208,7 +208,7 @@ def back_propogate(rays, ne_extent, probing_direction):
 
 
 # ---------------------------------------------------------------------------
-# Fixed-step RK4 trace (vectorised over rays)
+# Fixed-step Runge-Kutta-Nystrom trace (vectorised over rays)
 # ---------------------------------------------------------------------------
 class Grid:
     """Uniform grid with the fields the trace reads, in SI units: ne (m^-3),

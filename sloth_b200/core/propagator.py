@@ -9,9 +9,10 @@ Mirrors the reference's public functions (src/core/propagator.py):
 * ``trace_and_save_depths``                           (:932-1234)
 
 with the same signatures, return values and errors. The ODE is integrated
-with fixed-step RK4 (step = half the smallest grid spacing, in c*t) by the
-sm_100a tracers instead of diffrax's adaptive Tsit5, so ``jitted``,
-``parallelise``, ``rtol`` and ``atol`` are accepted and have no effect.
+with a fixed-step fourth-order Runge-Kutta-Nystrom method (step = half the
+smallest grid spacing, in c*t) by the sm_100a tracers instead of diffrax's
+adaptive Tsit5, so ``jitted``, ``parallelise``, ``rtol`` and ``atol`` are
+accepted and have no effect.
 Additive keyword-only extras: ``precision`` ('f32' = FP32 kernel with
 compensated sums and FP64 phase, 'f64' = all-FP64 kernel), ``detector_plane``
 (back-project the final rays to that plane), ``return_extras`` (append a dict

@@ -132,7 +132,7 @@ def sample(grid: DeviceGrid, points, *, stream=None) -> torch.Tensor:
 
 @dataclass
 class Schedule:
-    """Fixed-step RK4 schedule: every step is dtau (metres of c*t); save j is
+    """Fixed-step schedule: every step is dtau (metres of c*t); save j is
     taken after step first_save + j*save_every."""
     dtau: float
     first_save: int

@@ -96,7 +96,7 @@ def test_brems_geometry_amplitude_and_reference():
     amps = [float(np.asarray(a).mean()) for a in r['amplitude']]
     assert amps[-1] < 1.0
     assert all(amps[i] <= amps[i - 1] + 1e-6 for i in range(1, len(amps)))
-    # against the reference run (DOP853): the RK4 quadrature of the piecewise
+    # against the reference run (DOP853): the fixed-step quadrature of the piecewise
     # smooth kappa differs by ~1e-5 (see the oracle tests)
     np.testing.assert_allclose(np.stack(r['amplitude']), t["trough_ib_amp"], atol=2e-5)
     jv = np.asarray(r['jvec'][-1])

@@ -75,7 +75,7 @@ def test_jones_golden():
 
 
 # ---------------------------------------------------------------------------
-# Trajectories: the oracle's fixed-step RK4 against the reference's own
+# Trajectories: the oracle's fixed-step integrator against the reference's own
 # trace_and_save_depths / solve run with a tight DOP853 integrator.
 # ---------------------------------------------------------------------------
 def _trough_grid(ne0, n_xy, n_z, Te=None, Z=None):
@@ -111,7 +111,7 @@ def test_trough_matches_reference_and_analytic():
     sch = _depth_schedule(grid, t["trough_depths"])
     res = rr.trace_rays(grid, t["trough_s0"].astype(np.float64), **sch)
     x0 = np.array([0.5e-3, 1.0e-3, 1.5e-3, 2.0e-3])
-    # reference (DOP853) vs fixed-step RK4, and analytic SHM x0*cos(pi/4)
+    # reference (DOP853) vs the fixed-step integrator, and analytic SHM x0*cos(pi/4)
     _assert_jones(res["jones"][-1], t["trough_jvec"][-1], 2e-9, 2e-8)
     np.testing.assert_allclose(res["jones"][-1][0], x0 / np.sqrt(2), rtol=0, atol=2e-9)
     # vx = -x0*Omega*sin(pi/4) within the reference test's 10 %
@@ -126,7 +126,7 @@ def test_trough_inv_brems_matches_reference():
     res = rr.trace_rays(grid, t["trough_s0"].astype(np.float64), inv_brems=True, **sch)
     _assert_jones(res["jones"], t["trough_ib_jvec"], 5e-9, 2e-8)
     # kappa(r) along a path is only piecewise smooth (trilinear, kinks at cell
-    # faces): fixed-step RK4 quadrature differs from tight DOP853 by ~1e-5 here.
+    # faces): the fixed-step quadrature differs from tight DOP853 by ~1e-5 here.
     np.testing.assert_allclose(res["amp"], t["trough_ib_amp"], rtol=0, atol=2e-5)
 
 
