@@ -257,7 +257,7 @@ int sloth_trace_f32_noalloc(const SlothGridDesc* g, const void* grid, const Slot
 /* ---- K4/K5: detector image and its adjoint --------------------------------
  * No counterpart in the reference, which never differentiates. The forward
  * model maps the packed grid to a detector image:
- *   - fixed-step RK4 of the reference's ray equations (src/core/propagator.py
+ *   - fixed-step Runge-Kutta-Nystrom steps of the reference's ray equations (src/core/propagator.py
  *     168-243: dv/dt = -(c^2/2) grad(ne/nc), trilinear gradient, fill 0
  *     outside), at most n_steps steps of dtau, in the tracers' scaled scheme
  *     but without face clipping. A ray stops early once it is outside the
@@ -277,14 +277,14 @@ int sloth_trace_f32_noalloc(const SlothGridDesc* g, const void* grid, const Slot
  *     (same layout as the packed grid; the entry point zeroes it first;
  *     channel q stays 0);
  *   - it recomputes each checkpoint segment and runs the discrete adjoint of
- *     the RK4 steps in reverse.
+ *     the steps in reverse.
  * sloth_grid_pack_adjoint_* maps d L / d(packed grid) to d L / d ne through
  * the transpose of sloth_grid_pack_*: ne_grad = ne_scale * (dq + sum over
  * axes of the transposed difference stencil of the gradient channels).
  * _f32: FP32 grid, rays, image and compensated FP32 state (as sloth_trace_f32);
  * grid_grad accumulates with FP32 atomics. _f64: all FP64. */
 typedef struct SlothImageParams {
-    double  dtau;            /* RK4 step c*dt (m)                                  */
+    double  dtau;            /* step c*dt (m)                                      */
     int32_t n_steps;         /* steps per ray, at most                             */
     int32_t ckpt_every;      /* steps per checkpoint segment, 1 .. 32              */
     int32_t probing_axis;    /* detector plane normal: 0, 1 or 2                   */

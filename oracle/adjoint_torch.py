@@ -4,7 +4,7 @@ of the reference, which cannot run here because JAX is not installed. The
 device kernels are checked against it; the product never imports it.
 
 The model, in the tracers' scaled units (positions in grid cells, velocity
-in cells per step, one RK4 step = unit step):
+in cells per step, one step = unit step):
   * pack: q = ne * (1/nc); the gradient channels are dq/du per cell along each
     axis, central inside and one-sided on the faces. This is jnp.gradient
     with coordinates, as in precompute_gradients
@@ -13,7 +13,9 @@ in cells per step, one RK4 step = unit step):
     interpolation with cell i = floor(p) clamped to [0, n-2] and fill 0
     outside [0, n-1] (src/core/interpolator.py:79-104). This is dv/dt in
     dsdt (src/core/propagator.py:168-243) in scaled form.
-  * fixed-step RK4, at most n_steps steps. A ray stops once it is outside the
+  * fixed-step fourth-order Runge-Kutta-Nystrom steps (the tracers' method:
+    stages at p, p + w/2 + A1/8, p + w + A2/2; p' = p + w + (A1 + 2 A2)/6,
+    w' = w + (A1 + 4 A2 + A3)/6), at most n_steps. A ray stops once it is outside the
     grid on some axis and moving away from it along that axis; the check
     runs before each step.
   * straight line to the detector plane (src/shared/propagation.py:92-134);
@@ -86,7 +88,7 @@ def splat_profile(d: torch.Tensor, sigma: float) -> torch.Tensor:
 
 
 def final_states(ne, origin, spacing, omega, rays, *, dtau, n_steps):
-    """RK4 of every ray; returns (p, w) (N, 3) in cells, cells per step, and
+    """The steps of every ray; returns (p, w) (N, 3) in cells, cells per step, and
     the steps taken."""
     ne = ne.to(torch.float64)
     rays = torch.as_tensor(rays, dtype=torch.float64)
@@ -104,11 +106,10 @@ def final_states(ne, origin, spacing, omega, rays, *, dtau, n_steps):
         if not bool(alive.any()):
             break
         A1 = S * interp(ch, p)
-        A2 = S * interp(ch, p + 0.5 * w)
-        A3 = S * interp(ch, p + 0.5 * w + 0.25 * A1)
-        A4 = S * interp(ch, p + w + 0.5 * A2)
-        pn = p + w + (A1 + A2 + A3) / 6.0
-        wn = w + (A1 + 2.0 * A2 + 2.0 * A3 + A4) / 6.0
+        A2 = S * interp(ch, p + 0.5 * w + 0.125 * A1)
+        A3 = S * interp(ch, p + w + 0.5 * A2)
+        pn = p + w + (A1 + 2.0 * A2) / 6.0
+        wn = w + (A1 + 4.0 * A2 + A3) / 6.0
         m = alive[:, None]
         p = torch.where(m, pn, p)
         w = torch.where(m, wn, w)

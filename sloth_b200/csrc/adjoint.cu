@@ -8,11 +8,12 @@
 // 79-104, fill 0 outside) through a detector image:
 //
 //   ne --pack (K1)--> (q, dq/du, dq/dv, dq/dw)
-//      --fixed-step RK4, at most n_steps steps--> final ray state
+//      --fixed-step Runge-Kutta-Nystrom, at most n_steps steps--> final ray state
 //      --straight line to the detector plane--> (X, Y)
 //      --Gaussian splat--> image I
 //
-// RK4 is the tracer's scaled scheme (unit steps in grid cells) without face
+// The step is the tracer's (fourth-order Runge-Kutta-Nystrom, unit steps in
+// grid cells) without face
 // clipping: every stage samples the interpolant with fill 0 outside, so a
 // ray's map is smooth except where a stage point crosses a grid face. A ray
 // stops early once it is outside the grid on some axis and moving away from
@@ -30,7 +31,7 @@
 // gradient through the splat and the projection; then, segment by segment
 // from the last, the trajectory is recomputed from the segment's checkpoint
 // (the forward stores one every ckpt_every steps) and the discrete adjoint of
-// each RK4 step runs in reverse. Each stage's contribution to d L / d(grid
+// each step runs in reverse. Each stage's contribution to d L / d(grid
 // gradient channels) is accumulated in registers for the 8 corners of the
 // stage's cell and added to the grid-gradient buffer when the cell changes.
 // pack_adjoint_kernel maps d L / d(packed grid) through the transposed
@@ -247,14 +248,15 @@ __device__ __forceinline__ void accel(const ImageArgs& a, const typename P::R (&
     }
 }
 
-// One RK4 step (the tracer's rk4_step with phi = 1, without phase and depth):
-//   p' = p + w + (A1 + A2 + A3)/6,  w' = w + (A1 + 2A2 + 2A3 + A4)/6,
-//   stages at p, p + w/2, p + w/2 + A1/4, p + w + A2/2.
+// One step (the tracer's Runge-Kutta-Nystrom step with phi = 1, without
+// phase and depth):
+//   p' = p + w + (A1 + 2 A2)/6,  w' = w + (A1 + 4 A2 + A3)/6,
+//   stages at p, p + w/2 + A1/8, p + w + A2/2.
 template <class P, bool INTERIOR = false, class Cell>
 __device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, Cell& cc,
                                            typename P::R* A1out = nullptr, typename P::R* A2out = nullptr) {
     using R = typename P::R;
-    R ph[3], pl[3], we[3], st[3], A1[3], A2[3], A3[3], A4[3];
+    R ph[3], pl[3], we[3], st[3], A1[3], A2[3], A3[3];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         ph[x] = r.p[x].hi();
@@ -263,14 +265,11 @@ __device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, Cel
     }
     accel<P, INTERIOR>(a, ph, pl, A1, cc);
 #pragma unroll
-    for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * we[x];
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + (R(0.5) * we[x] + R(0.125) * A1[x]);
     accel<P, INTERIOR>(a, ph, st, A2, cc);
 #pragma unroll
-    for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * (we[x] + R(0.5) * A1[x]);
-    accel<P, INTERIOR>(a, ph, st, A3, cc);
-#pragma unroll
     for (int x = 0; x < 3; ++x) st[x] = pl[x] + (we[x] + R(0.5) * A2[x]);
-    accel<P, INTERIOR>(a, ph, st, A4, cc);
+    accel<P, INTERIOR>(a, ph, st, A3, cc);
     if (A1out) {
 #pragma unroll
         for (int x = 0; x < 3; ++x) {
@@ -280,15 +279,15 @@ __device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, Cel
     }
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
-        const R sA = (A1[x] + A2[x]) + A3[x];
-        const R sW = ((A1[x] + R(2) * A2[x]) + R(2) * A3[x]) + A4[x];
+        const R sA = A1[x] + R(2) * A2[x];
+        const R sW = (A1[x] + R(4) * A2[x]) + A3[x];
         r.p[x].add(r.w[x].hi() + (r.w[x].lo() + sA * R(1.0 / 6.0)));
         r.w[x].add(sW * R(1.0 / 6.0));
     }
 }
 
 // ---------------------------------------------------------------------------
-// Adjoint of one RK4 step.
+// Adjoint of one step.
 // ---------------------------------------------------------------------------
 template <class P>
 struct CornerAcc {
@@ -435,45 +434,36 @@ __device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const MSt
         pl[x] = r.p[x].lo();
         we[x] = r.w[x].val();
     }
-    // A1, A2 (which place stages 3 and 4) come from the segment's recompute
-    R a1[3], a2[3], a3[3], a4[3], pb[3], wb[3], q[3];
+    // A1, A2 (which place stages 2 and 3) come from the segment's recompute.
+    // Direct terms of p' = p + w + (A1 + 2 A2)/6, w' = w + (A1 + 4 A2 + A3)/6:
+    R a1[3], a2[3], a3[3], pb[3], wb[3], q[3];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         a1[x] = (lp[x] + lw[x]) * R(1.0 / 6.0);
-        a2[x] = lp[x] * R(1.0 / 6.0) + lw[x] * R(1.0 / 3.0);
-        a3[x] = a2[x];
-        a4[x] = lw[x] * R(1.0 / 6.0);
+        a2[x] = lp[x] * R(1.0 / 3.0) + lw[x] * R(2.0 / 3.0);
+        a3[x] = lw[x] * R(1.0 / 6.0);
         pb[x] = lp[x];
         wb[x] = lp[x] + lw[x];
     }
-    // stage 4 at p + w + A2/2
+    // stage 3 at p + w + A2/2
 #pragma unroll
     for (int x = 0; x < 3; ++x) st[x] = pl[x] + (we[x] + R(0.5) * A2[x]);
-    stage_adjoint<P>(a, ph, st, a4, q, cc, acc);
+    stage_adjoint<P>(a, ph, st, a3, q, cc, acc);
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         pb[x] += q[x];
         wb[x] += q[x];
         a2[x] += R(0.5) * q[x];
     }
-    // stage 3 at p + w/2 + A1/4
+    // stage 2 at p + w/2 + A1/8
 #pragma unroll
-    for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * (we[x] + R(0.5) * A1[x]);
-    stage_adjoint<P>(a, ph, st, a3, q, cc, acc);
-#pragma unroll
-    for (int x = 0; x < 3; ++x) {
-        pb[x] += q[x];
-        wb[x] += R(0.5) * q[x];
-        a1[x] += R(0.25) * q[x];
-    }
-    // stage 2 at p + w/2
-#pragma unroll
-    for (int x = 0; x < 3; ++x) st[x] = pl[x] + R(0.5) * we[x];
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + (R(0.5) * we[x] + R(0.125) * A1[x]);
     stage_adjoint<P>(a, ph, st, a2, q, cc, acc);
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         pb[x] += q[x];
         wb[x] += R(0.5) * q[x];
+        a1[x] += R(0.125) * q[x];
     }
     // stage 1 at p
     stage_adjoint<P>(a, ph, pl, a1, q, cc, acc);

@@ -1,8 +1,8 @@
 """CPU checks of the detector-image oracle (oracle/adjoint_torch.py), the
-reference the adjoint kernels are tested against: its RK4 converges at
-fourth order to the tracer oracle (which is pinned to the reference's golden
-vectors) away from the faces, it integrates a linear density ramp exactly,
-and its autograd gradient equals its own central differences."""
+reference the adjoint kernels are tested against: its steps equal the tracer
+oracle's (which is pinned to the reference's golden vectors) away from the
+faces, it integrates a linear density ramp exactly, and its autograd
+gradient equals its own central differences."""
 import math
 
 import numpy as np
@@ -17,38 +17,33 @@ L = 5e-3
 LWL = 532e-9
 
 
-def test_rk4_converges_to_the_tracer_oracle_inside_the_grid():
-    """The detector model integrates with classical RK4; the tracer oracle
-    with the fourth-order Runge-Kutta-Nystrom method. Both discretise the same
-    ray equation, so on rays that stay inside the grid their difference must
-    shrink as the fourth power of the step: about 16x per halving."""
+def test_steps_match_the_tracer_oracle_inside_the_grid():
+    """The detector model steps like the tracer oracle (which is pinned to the
+    reference's golden vectors): on rays that stay inside the grid, their
+    states agree to rounding."""
     n = 20
     h = L / (n - 1)
     ne = workloads.kolmogorov_box(n, L=L, mean=2e26, rms=0.3, seed=4).double()
     om = physics.omega_of(LWL)
-    # rays that start deep inside and stay there over the traced time
+    # rays that start deep inside and stay there for 12 steps
     g = torch.Generator().manual_seed(1)
     rays = torch.zeros(6, 64, dtype=torch.float64)
     rays[0:3] = (torch.rand(3, 64, generator=g, dtype=torch.float64) - 0.5) * (0.4 * L)
     d = torch.randn(3, 64, generator=g, dtype=torch.float64)
     rays[3:6] = d / d.norm(dim=0) * at.C
+    dtau, steps = h / 2, 12
+    p, w, taken = at.final_states(ne, (-L / 2,) * 3, (h,) * 3, om, rays, dtau=dtau, n_steps=steps)
+    assert int(taken.min()) == steps
     grid = rr.Grid(ne.numpy(), (-L / 2,) * 3, (h,) * 3, om)
-    diffs = []
-    for k in (2, 4, 8):
-        dtau, steps = h / k, 6 * k
-        p, w, taken = at.final_states(ne, (-L / 2,) * 3, (h,) * 3, om, rays, dtau=dtau, n_steps=steps)
-        assert int(taken.min()) == steps
-        ref = rr.trace_rays(grid, rays.numpy(), dtau=dtau, first_save=steps, save_every=1, n_saves=1)["state"][0]
-        pos = p.numpy().T * h - L / 2
-        vel = w.numpy().T * at.C * h / dtau
-        diffs.append((np.abs(pos - ref[:3]).max() / L, np.abs(vel - ref[3:]).max() / at.C))
-    assert diffs[0][0] < 1e-9 and diffs[0][1] < 1e-8, diffs
-    for a, b in zip(diffs, diffs[1:]):
-        assert a[0] / b[0] > 12 and a[1] / b[1] > 12, diffs
+    ref = rr.trace_rays(grid, rays.numpy(), dtau=dtau, first_save=steps, save_every=1, n_saves=1)["state"][0]
+    pos = p.numpy().T * h - L / 2
+    vel = w.numpy().T * at.C * h / dtau
+    np.testing.assert_allclose(pos, ref[:3], rtol=0, atol=1e-13 * L)
+    np.testing.assert_allclose(vel, ref[3:], rtol=1e-11, atol=1e-6)
 
 
 def test_linear_ramp_is_integrated_exactly():
-    # ne = n0 (1 + x/Lr): constant gradient, so RK4 reproduces the parabola
+    # ne = n0 (1 + x/Lr): constant gradient, so the step reproduces the parabola
     n, n0, Lr = 24, 1e26, 2e-3
     h = L / (n - 1)
     x = -L / 2 + h * torch.arange(n, dtype=torch.float64)
