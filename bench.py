@@ -286,7 +286,7 @@ def run_diagnostics(outs):
 
 # ---------------------------------------------------------------------------
 # adjoint: d loss / d ne for a 256^2 detector image of 1e6 rays through a
-# 128^3 FP32 Kolmogorov grid (400 RK4 steps, checkpoints every 20, 2-pixel
+# 128^3 FP32 Kolmogorov grid (400 steps, checkpoints every 20, 2-pixel
 # splat); loss = ||I - I_target||^2 with I_target from another seeded field
 # ---------------------------------------------------------------------------
 def run_adjoint(args):
@@ -339,7 +339,7 @@ def run_adjoint(args):
         ad.append(float(g32[v]))
     fd, ad = np.array(fd), np.array(ad)
     fms, bms = float(np.median(fwd_ms)), float(np.median(bwd_ms))
-    out = {"workload": "128^3 FP32 Kolmogorov grid, 1e6 rays (3 mm Gaussian beam), 400 RK4 steps, checkpoints "
+    out = {"workload": "128^3 FP32 Kolmogorov grid, 1e6 rays (3 mm Gaussian beam), 400 steps, checkpoints "
                        "every 20, 256^2 detector, 2-pixel Gaussian splat, L = ||I - I_target||^2",
            "ray_steps": steps, "forward_ms": fms, "backward_ms": bms,
            "forward_ray_steps_per_s": steps / (fms / 1e3), "backward_ray_steps_per_s": steps / (bms / 1e3),

@@ -8,10 +8,11 @@ synthetic detector image (see include/sloth_b200.h, "K4/K5"):
     loss = ((image - target) ** 2).sum()
     loss.backward()          # ne.grad from the hand-written adjoint kernels
 
-Forward: K1 packs ne, K4 traces every ray with fixed-step RK4 (checkpointing
+Forward: K1 packs ne, K4 traces every ray with fixed-step Runge-Kutta-Nystrom
+steps (checkpointing
 its state every ``spec.ckpt_every`` steps) and splats its detector point.
 Backward: K5 recomputes each checkpoint segment and runs the discrete adjoint
-of the RK4 steps in reverse into d loss / d(packed grid); the pack adjoint
+of the steps in reverse into d loss / d(packed grid); the pack adjoint
 maps that to d loss / d ne. All on the GPU through the C ABI; there is no CPU
 path.
 """
@@ -33,7 +34,7 @@ class DetectorSpec:
     """Detector plane, image and integration settings of the forward model."""
     window: Tuple[float, float, float, float]   # u0, u1, v0, v1 (m) on the transverse axes (ascending)
     plane: float                                # detector plane along `axis` (m)
-    dtau: float                                 # RK4 step c*dt (m)
+    dtau: float                                 # step c*dt (m)
     n_px: Tuple[int, int] = (256, 256)
     axis: int = 2
     sigma_px: float = 2.0
@@ -158,7 +159,7 @@ def detector_image(ne: torch.Tensor, rays: torch.Tensor, spec: DetectorSpec, *, 
                    precision: str = "f32", stats: Optional[dict] = None, group=None) -> torch.Tensor:
     """The detector image of `rays` (6, N) through the density `ne` (m^-3);
     differentiable with respect to `ne`. If `stats` is a dict, its
-    "ray_steps" entry receives a device counter of the RK4 steps taken (this
+    "ray_steps" entry receives a device counter of the steps taken (this
     process's rays). With a torch.distributed process group, each rank passes
     its share of the rays and gets the image and the gradient of all of them
     (see DetectorImage)."""
