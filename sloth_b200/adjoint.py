@@ -9,8 +9,8 @@ synthetic detector image (see include/sloth_b200.h, "K4/K5"):
     loss.backward()          # ne.grad from the hand-written adjoint kernels
 
 Forward: K1 packs ne, K4 traces every ray with fixed-step Runge-Kutta-Nystrom
-steps (checkpointing
-its state every ``spec.ckpt_every`` steps) and splats its detector point.
+steps (checkpointing its state every ``spec.ckpt_every`` steps) and splats its
+detector point.
 Backward: K5 recomputes each checkpoint segment and runs the discrete adjoint
 of the steps in reverse into d loss / d(packed grid); the pack adjoint
 maps that to d loss / d ne. All on the GPU through the C ABI; there is no CPU
