@@ -21,7 +21,7 @@ constexpr double kC = 299792458.0;          // speed of light (scipy.constants.c
 constexpr int kTile = 1024;                 // rays per shared-memory sorted tile
 constexpr int kSmallTile = 256;             // rays per tile at the end of a trace's tile queue
 #ifndef SLOTH_TAIL_WAVES
-#define SLOTH_TAIL_WAVES 16
+#define SLOTH_TAIL_WAVES 32
 #endif
 constexpr int kTailWaves = SLOTH_TAIL_WAVES;  // small tiles per CTA at the end of the queue
 constexpr int kMaxBucketBits = 18;          // at most 2^18 Morton buckets

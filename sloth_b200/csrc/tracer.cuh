@@ -771,7 +771,7 @@ __device__ __forceinline__ int step_kind(const TraceArgs& a, const Ray<P>& r, ty
 
 // Number of steps after the current interior step (kind 0) that are certainly
 // kind 0 too, for a trace whose accelerations are bounded by B =
-// a.accel_bound: 63, 15, 3 or 0. From the state (p, w) now, after j steps
+// a.accel_bound: 127, 31, 7 or 0. From the state (p, w) now, after j steps
 // |w_j - w| <= j B (each step adds a weighted mean of stage accelerations)
 // and |p_j - p - j w| <= B j^2 / 2 (each step moves w_i + (A1 + A2 + A3) / 6),
 // so the position p_j and the prediction p_j + w_j lie within
@@ -800,9 +800,9 @@ __device__ __forceinline__ int interior_run(const TraceArgs& a, const Ray<P>& r)
         }
         return ok;
     };
-    if (fits(63)) return 63;
-    if (fits(15)) return 15;
-    if (fits(3)) return 3;
+    if (fits(127)) return 127;
+    if (fits(31)) return 31;
+    if (fits(7)) return 7;
     return 0;
 }
 

@@ -24,7 +24,7 @@ def _rkn_step(p, w, accel):
 
 
 @pytest.mark.parametrize("mode", ["random", "push", "alternate"])
-@pytest.mark.parametrize("m", [3, 7, 15, 31, 63])
+@pytest.mark.parametrize("m", [3, 7, 15, 31, 63, 127])
 def test_run_envelope_holds(mode, m):
     rng = np.random.default_rng(1 + m)
     B = 0.03
