@@ -7,7 +7,8 @@ C ABI, against the oracle:
   lattice. The grid is the configuration's; the rays are every 50th lattice
   ray, so that the FP64 oracle finishes in seconds;
 * a 128^3 Kolmogorov box with inverse bremsstrahlung, the headline mode at
-  a size the oracle can follow.
+  a size the oracle can follow;
+* 40 saves a few steps apart, which the tracer's interior runs must stop at.
 
 The trough also has an analytic answer: its transverse motion is simple
 harmonic, x(t) = x0 cos(W t) + (vx0 / W) sin(W t) with W = c sqrt(n0/nc) / Lp,
@@ -102,4 +103,25 @@ def test_kolmogorov_128_with_absorption(precision):
     assert dph[:, ~side].max() <= _tol(precision) * ph
     damp = np.abs(k["amp"].astype(np.float64) - o["amp"])
     assert damp[:, ~side].max() < (1e-12 if precision == "f64" else 1e-6)
+    assert (k["steps"] != o["steps"]).mean() < 1e-3
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_many_saves_inside_interior_runs(precision):
+    """40 saves, every few steps: the tracer's uniform step loop must stop at
+    each save inside its interior runs. Against the oracle at every save."""
+    n = 48
+    h = L / (n - 1)
+    ne = workloads.kolmogorov_box(n, L=L, mean=1e25, rms=0.2, seed=41).numpy()
+    rays = workloads.gaussian_beam(3000, waist=1.5e-3, L=L, seed=42).numpy()
+    sched = runtime.schedule_times(np.linspace(0.0, 1.2 * L, 40), (h, h, h))
+    assert sched.n_saves == 40 and sched.save_every >= 2
+    kw = dict(inv_brems=True, Te=20.0, Z=1.0)
+    k = run_kernel(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched, precision=precision, **kw)
+    o = run_oracle(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched, **kw)
+    assert position_error(k["state"], o["state"], L) < _tol(precision)
+    assert direction_error(k["state"], o["state"]) < _tol(precision)
+    inside = np.all(np.abs(o["state"][:, :2]) <= L / 2, axis=1)      # (saves, rays) off the side faces
+    ph = np.abs(o["phase"]).max()
+    assert np.abs(k["phase"] - o["phase"])[inside].max() <= _tol(precision) * ph
     assert (k["steps"] != o["steps"]).mean() < 1e-3
