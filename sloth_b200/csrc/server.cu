@@ -96,10 +96,10 @@ serve_kernel(const TraceArgs* __restrict__ table, WorkHeader* hdr, const WorkIte
         const int cnt = (int)min((long long)kTile, s_args.n - start);
         unsigned long long my_steps = 0;
         // the job's density range bounds its accelerations: the interior fast path
-        if (s_args.accel_bound > 0.0f)
-            trace_tile<PolF32, IB, SMALLX, true>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
+        if (interior_sampling_ok(s_args))
+            trace_tile<PolF32, IB, SMALLX, 1>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
         else
-            trace_tile<PolF32, IB, SMALLX, false>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
+            trace_tile<PolF32, IB, SMALLX, 0>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
         block_add(my_steps, &s_steps, s_args.total_steps);
     }
 }

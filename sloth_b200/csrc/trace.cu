@@ -7,7 +7,7 @@
 
 namespace sloth {
 
-template <class P, int IB, bool SMALLX, bool FAST>
+template <class P, int IB, bool SMALLX, int FAST>
 __global__ void __launch_bounds__(kThreads, SLOTH_TRACE_MIN_BLOCKS)
 trace_kernel(const __grid_constant__ TraceArgs a) {
     __shared__ unsigned s_key[kTile];
@@ -45,7 +45,7 @@ trace_kernel(const __grid_constant__ TraceArgs a) {
     block_add(my_steps, &s_steps, a.total_steps);
 }
 
-template <class P, int IB, bool SMALLX, bool FAST>
+template <class P, int IB, bool SMALLX, int FAST>
 static int launch_trace_k(const TraceArgs& ta, int sms, cudaStream_t s) {
     static int cached[64] = {0};
     int dev = 0;
@@ -72,8 +72,10 @@ static int launch_trace_k(const TraceArgs& ta, int sms, cudaStream_t s) {
 }
 
 template <class P, int IB, bool SMALLX>
-static int launch_trace(const TraceArgs& ta, int sms, cudaStream_t s, bool fast) {
-    return fast ? launch_trace_k<P, IB, SMALLX, true>(ta, sms, s) : launch_trace_k<P, IB, SMALLX, false>(ta, sms, s);
+static int launch_trace(const TraceArgs& ta, int sms, cudaStream_t s, int fast) {
+    return fast == 1 ? launch_trace_k<P, IB, SMALLX, 1>(ta, sms, s)
+         : fast == 2 ? launch_trace_k<P, IB, SMALLX, 2>(ta, sms, s)
+                     : launch_trace_k<P, IB, SMALLX, 0>(ta, sms, s);
 }
 
 template <class P>
@@ -126,7 +128,8 @@ static int trace_impl(const SlothGridDesc* g, const void* grid, const SlothTrace
     int ib;
     bool smallx;
     trace_mode(p, &ib, &smallx);
-    const bool fast = interior_bound_ok(g, p);
+    // interior runs with interior sampling, interior runs only, or neither
+    const int fast = interior_bound_ok(g, p) ? 1 : (std::isfinite(interior_accel_bound(g, p)) ? 2 : 0);
 
     if (out->trace_event_begin) {
         e = cudaEventRecord((cudaEvent_t)out->trace_event_begin, s);

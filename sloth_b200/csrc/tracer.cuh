@@ -96,8 +96,8 @@ struct TraceArgs {
     float Sf[3];               // the same, rounded to FP32 once here (the FP32 tracer reads these
                                // instead of converting the doubles inside its loop)
     float ope2f, cl_lof, cl_wf;
-    float accel_bound;         // bound on |acceleration| (cells per step^2) when it permits the
-                               // interior fast path, else 0 (see interior_run)
+    float accel_bound;         // bound on |acceleration| (cells per step^2), 0 when unknown
+                               // (see interior_run and interior_sampling_ok)
     double phase_scale;        // (omega/c) * dtau / 6
     double tau_scale;          // kappa_q2 * dtau / 6
     double cl_w, cl_lo;        // Coulomb log below nc, and max(2, cl_w)
@@ -806,6 +806,13 @@ __device__ __forceinline__ int interior_run(const TraceArgs& a, const Ray<P>& r)
     return 0;
 }
 
+// Whether a trace's interior steps may sample without the grid test: its
+// accelerations are bounded by kInteriorAccel (accel_bound carries 0.1% of
+// headroom over the bound).
+__device__ __forceinline__ bool interior_sampling_ok(const TraceArgs& a) {
+    return a.accel_bound > 0.0f && a.accel_bound <= (float)(kInteriorAccel * 1.001);
+}
+
 template <class P>
 __device__ __forceinline__ bool ray_in_grid(const TraceArgs& a, const Ray<P>& r) {
     using R = typename P::R;
@@ -976,7 +983,11 @@ __device__ __forceinline__ void tile_sort(unsigned* key, unsigned* id, int size)
 // trace them one thread per ray, refilling finished lanes from the tile
 // (warp ballot + shared-memory atomic). *s_head must be 0 on entry and the
 // block must be synchronised. Shared by the single-trace and serving kernels.
-template <class P, int IB, bool SMALLX, bool FAST, class Cache>
+// FAST: 0 every step runs the face test; 1 steps proven interior by the
+// acceleration bound skip it and sample without the grid test (bound at most
+// kInteriorAccel); 2 they skip the face test but sample with the grid test
+// (any finite bound). Every mode takes the same steps.
+template <class P, int IB, bool SMALLX, int FAST, class Cache>
 __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, int cnt, unsigned* s_key,
                                            unsigned* s_id, int* s_head, Cache& cc,
                                            unsigned long long& my_steps) {
@@ -1041,7 +1052,8 @@ __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, 
             if (FAST && kind == 0) {
 #pragma unroll 1
                 for (int e = 0;; ++e) {
-                    step_any<P, IB, SMALLX, SAMPLE_INTERIOR, true>(a, r, cc, typename P::R(1));
+                    step_any<P, IB, SMALLX, FAST == 1 ? SAMPLE_INTERIOR : SAMPLE_PLAIN, true>(a, r, cc,
+                                                                                            typename P::R(1));
                     if (e == extra) break;
                     ++r.step;
                 }
@@ -1328,7 +1340,7 @@ inline void fill_trace_args(TraceArgs& ta, const SlothGridDesc* g, const void* g
     ta.cl_wf = (float)ta.cl_w;
     {
         const double B = interior_accel_bound(g, p);
-        ta.accel_bound = B <= kInteriorAccel ? (float)(B * 1.001) : 0.0f;
+        ta.accel_bound = std::isfinite(B) ? (float)(B * 1.001) : 0.0f;
     }
     ta.plane = p->plane;
     ta.first_save = p->first_save;

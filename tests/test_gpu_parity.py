@@ -18,7 +18,7 @@ import torch
 from conftest import golden
 from helpers import C, case, direction_error, position_error, run_kernel, run_oracle
 from oracle import ref_restated as rr
-from sloth_b200 import _capi, runtime
+from sloth_b200 import _capi, runtime, workloads
 
 pytestmark = pytest.mark.gpu
 
@@ -266,3 +266,40 @@ def test_interior_fast_path_is_bitwise_identical(precision):
             f, s_ = fast[key].double(), slow[key].double()
             scale = s_.abs().amax(dim=-1, keepdim=True).clamp_min(1e-300)
             assert float(((f - s_).abs() / scale).max()) < 1e-12, key
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_dense_plasma_interior_runs(precision):
+    """A density near 0.4 nc bounds the accelerations above the interior
+    sampling limit (0.03 cells per step^2), so the tracer keeps the grid test
+    on every stage but still skips the face test on runs of steps proven
+    interior. The results must equal the kernel without any fast path (FP32
+    bitwise, FP64 to rounding) and the oracle."""
+    import dataclasses
+    n = 48
+    h = L / (n - 1)
+    ne = workloads.kolmogorov_box(n, L=L, mean=1.5e27, rms=0.2, seed=51).numpy()
+    rays = workloads.gaussian_beam(3000, waist=1.5e-3, L=L, seed=52, jitter=2e-3).numpy()
+    omega = 2 * np.pi * C / 532e-9
+    sched = _sched(n, 3, False)
+    g = runtime.pack_grid(torch.from_numpy(ne), (-L / 2,) * 3, (h,) * 3, omega, precision=precision)
+    bound = 0.5 * (sched.dtau / h) ** 2 * (g.q_max - min(g.q_min, 0.0))
+    assert 0.03 < bound < 1.0
+    dt = torch.float32 if precision == "f32" else torch.float64
+    r = torch.from_numpy(rays).to("cuda", dt)
+    kw = dict(project=True, plane=L / 2, inv_brems=True, Te=20.0, Z=1.0, want_state=True)
+    runs = runtime.trace(g, r, sched, **kw)
+    plain = runtime.trace(dataclasses.replace(g, q_min=float("inf")), r, sched, **kw)
+    torch.cuda.synchronize()
+    for key in ("jones", "state", "phase", "amp", "status", "steps", "total_steps"):
+        if precision == "f32" or key in ("status", "steps", "total_steps"):
+            assert torch.equal(runs[key], plain[key]), key
+        else:
+            f, s_ = runs[key].double(), plain[key].double()
+            scale = s_.abs().amax(dim=-1, keepdim=True).clamp_min(1e-300)
+            assert float(((f - s_).abs() / scale).max()) < 1e-12, key
+    k = {kk: v.cpu().numpy() for kk, v in runs.items()}
+    o = run_oracle(ne, rays, (-L / 2,) * 3, (h,) * 3, omega, sched, **{kk: kw[kk] for kk in ("project", "plane", "inv_brems", "Te", "Z")})
+    tol = 1e-10 if precision == "f64" else 1e-6
+    assert position_error(k["state"], o["state"], L) < tol
+    assert direction_error(k["state"], o["state"]) < tol
