@@ -85,13 +85,13 @@ typedef struct SlothTraceParams {
                                  kappa; series n - 1 when (omega_pe/omega)^2 <= 0.05) */
     double  q_min;            /* lower bound of ne/nc over the grid (0 for a density
                                  known to be >= 0). With q_max it bounds the ray's
-                                 acceleration; when that bound keeps every stage point
-                                 of an interior step inside the grid, those steps skip
-                                 the per-stage grid test, and runs of steps proven
-                                 interior skip the face test (bitwise the same results
-                                 in FP32, within 1e-12 relative in FP64; fewer
-                                 instructions). A value above the true minimum is an
-                                 error of the caller. */
+                                 acceleration. Runs of steps that the bound proves
+                                 interior skip the face test; when the bound also keeps
+                                 every stage point of an interior step inside the grid,
+                                 those steps skip the per-stage grid test as well
+                                 (bitwise the same results in FP32, within 1e-12
+                                 relative in FP64; fewer instructions). A value above
+                                 the true minimum is an error of the caller. */
 } SlothTraceParams;
 
 #define SLOTH_MAX_SAVES 4096
