@@ -110,3 +110,31 @@ def test_short_request_stream():
     assert res["requests"] == 40
     assert res["p99_ms"] >= res["p50_ms"] > 0
     assert res["ray_steps"] > 0 and res["stats"]["iterations"] >= 1
+
+
+def test_dense_job_in_the_mix_with_fast_path_jobs():
+    """A dense job (near 0.4 nc: its accelerations exceed the interior
+    sampling limit) shares the server's kernels with jobs that take the
+    interior fast path. Each job's rays must be bitwise its single-trace
+    rays, whose dense trace takes interior runs with the grid test."""
+    specs = [("kolmogorov", 48, 5000, 1), ("sinusoid", 64, 3000, 2)]
+    fields = _fields(specs)
+    n = 40
+    h = L / (n - 1)
+    dkey = serving.grid_key("kolmogorov", n, 99)
+    fields[dkey] = workloads.kolmogorov_box(n, L=L, mean=1.5e27, rms=0.2, seed=9, device="cuda")
+    rays_d = workloads.gaussian_beam(4000, waist=2e-3, L=L, seed=7, jitter=1e-3, device="cuda")
+    with serving.RayServer(2 << 30, tiles_per_step=64, quantum=2) as srv:
+        jobs = [_submit(srv, fields, k, nn, nr, s) for k, nn, nr, s in specs]
+        jd = srv.submit(dkey, fields[dkey], (-L / 2,) * 3, (h,) * 3, (n,) * 3, rays_d, lwl=LWL,
+                        detector_plane=L / 2, inv_brems=True, Te=20.0, Z=1.0)
+        srv.run_until_done([j for j, _ in jobs] + [jd])
+        outs = [j.out for j, _ in jobs] + [jd.out]
+    for (kind, nn, _, _), (job, rays), out in zip(specs, jobs, outs):
+        _same(out, _direct(fields, kind, nn, rays))
+    g = runtime.pack_grid(fields[dkey], (-L / 2,) * 3, (h,) * 3, physics.omega_of(LWL))
+    sched = runtime.schedule_times([math.sqrt(8.0) * L], (h, h, h))
+    assert 0.5 * (sched.dtau / h) ** 2 * (g.q_max - min(g.q_min, 0.0)) > 0.03
+    direct = runtime.trace(g, rays_d, sched, project=True, plane=L / 2, inv_brems=True, Te=20.0, Z=1.0)
+    torch.cuda.synchronize()
+    _same(outs[-1], {k: v.cpu() for k, v in direct.items()})
