@@ -41,3 +41,25 @@ def test_ctypes_structs_match_the_c_header(tmp_path):
         name, _, field = key.partition(".")
         got[(name, field)] = int(value)
     assert got == expected
+
+
+def test_integration_stub_structs_match_the_binding():
+    """The ctypes stub that INTEGRATION.md shows a SLOTH maintainer declares
+    the same struct layouts as the binding (its class definitions run here;
+    the library loading lines do not)."""
+    import re
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```python\n(.*?)```", text, flags=re.S)
+    stub = next(b for b in blocks if "class TraceParams(Structure)" in b)
+    import ast
+    tree = ast.parse(stub)
+    keep = [n for n in tree.body if isinstance(n, (ast.Import, ast.ImportFrom, ast.ClassDef))]
+    ns = {}
+    exec(compile(ast.Module(body=keep, type_ignores=[]), "INTEGRATION.md", "exec"), ns)
+    for stub_name, name in (("GridDesc", "SlothGridDesc"), ("TraceParams", "SlothTraceParams"),
+                            ("TraceOutputs", "SlothTraceOutputs")):
+        a, b = ns[stub_name], getattr(_capi, name)
+        assert _capi.ctypes.sizeof(a) == _capi.ctypes.sizeof(b), stub_name
+        assert [f for f, _ in a._fields_] == [f for f, _ in b._fields_], stub_name
+        for f, _ in a._fields_:
+            assert getattr(a, f).offset == getattr(b, f).offset, (stub_name, f)
