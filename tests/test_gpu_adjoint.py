@@ -146,7 +146,8 @@ def test_error_codes():
 
 
 def test_gradient_against_finite_differences_128cube_1e6_rays():
-    """The 128^3 FP32 grid, 1e6 rays, 400 RK4 steps with checkpoints every
+    """The 128^3 FP32 grid, 1e6 rays, 400 fourth-order steps (the tracer's
+    Runge-Kutta-Nystrom step) with checkpoints every
     20, 256^2 image with a 2-pixel splat: d L / d ne from the FP32 adjoint
     against central differences of the FP64 forward at 64 random voxels of
     the beam's core."""
