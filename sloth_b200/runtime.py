@@ -288,18 +288,21 @@ def _chunk_bounds(n: int, cs: int) -> list:
     """Chunk boundaries of n rays for trace_to_host: about `cs` rays per
     chunk, but the first and the last chunk hold only STREAM_END_RAYS (when
     cs is larger), because the first chunk's copy in and the last chunk's
-    copy out are the only copies no trace hides."""
+    copy out are the only copies no trace hides. Chunks between the ends
+    differ in size by one ray at most."""
     if n <= 0:
         return [0, 0]
+
+    def split(lo, hi):
+        m = hi - lo
+        k = max(1, -(-m // cs))
+        q, r = divmod(m, k)
+        return [lo + i * q + min(i, r) for i in range(k + 1)]
+
     end = min(cs, STREAM_END_RAYS)
     if n <= 2 * end + cs:
-        k = max(1, -(-n // cs))
-        c = -(-n // k)
-        return [min(n, i * c) for i in range(k + 1)]
-    mid = n - 2 * end
-    k = -(-mid // cs)
-    c = -(-mid // k)
-    return [0] + [min(n - end, end + i * c) for i in range(k + 1)] + [n]
+        return split(0, n)
+    return [0] + split(end, n - end) + [n]
 
 
 def trace_to_host(grid: DeviceGrid, rays, sched: Schedule, *, want: dict, chunk_rays: Optional[int] = None,
