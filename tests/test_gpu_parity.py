@@ -303,3 +303,42 @@ def test_dense_plasma_interior_runs(precision):
     tol = 1e-10 if precision == "f64" else 1e-6
     assert position_error(k["state"], o["state"], L) < tol
     assert direction_error(k["state"], o["state"]) < tol
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_nonfinite_rays_are_flagged_and_leave_the_others_unchanged(precision):
+    """Rays whose position or direction holds NaN or Inf end with status
+    SLOTH_RAY_NONFINITE and non-finite outputs. The finite rays traced in the
+    same launch get bitwise the results they get without them. (The Morton
+    keys clamp such coordinates into the grid, and the samplers' index clamps
+    keep every grid access inside it, so these rays only waste their steps.)"""
+    ne, rays, origin, spacing, omega = case("kolmogorov", 40, 512, seed=5)
+    sched = _sched(40, 3, False)
+    dt = torch.float32 if precision == "f32" else torch.float64
+    bad = rays.astype(np.float64)
+    picks = {3: (0, np.nan), 17: (4, np.nan), 64: (2, np.inf), 100: (1, -np.inf), 200: (5, np.inf),
+             300: (3, -np.inf)}
+    for ray, (row, value) in picks.items():
+        bad[row, ray] = value
+    idx = np.array(sorted(picks))
+    good = np.setdiff1d(np.arange(rays.shape[1]), idx)
+    g = runtime.pack_grid(torch.from_numpy(ne), origin, spacing, omega, precision=precision)
+    kw = dict(inv_brems=True, Te=20.0, Z=1.0, want_state=True, want_status=True, want_steps=True)
+    mixed = runtime.trace(g, torch.from_numpy(bad).to("cuda", dt), sched, **kw)
+    alone = runtime.trace(g, torch.from_numpy(np.ascontiguousarray(bad[:, good])).to("cuda", dt), sched, **kw)
+    torch.cuda.synchronize()
+    m = {k: v.cpu().numpy() for k, v in mixed.items()}
+    a = {k: v.cpu().numpy() for k, v in alone.items()}
+    assert (m["status"][idx] == _capi.SLOTH_RAY_NONFINITE).all(), m["status"][idx]
+    assert (m["status"][good] != _capi.SLOTH_RAY_NONFINITE).all()
+    assert not np.isfinite(m["state"][-1][:, idx]).all(axis=0).any()
+    for key in ("jones", "state", "phase", "amp"):
+        if precision == "f32":
+            np.testing.assert_array_equal(m[key][..., good], a[key])
+        else:   # FP64 is held to 1e-12 of the output's scale, as in the fast-path test
+            scale = np.abs(a[key]).max()
+            assert np.abs(m[key][..., good] - a[key]).max() <= 1e-12 * scale, key
+    np.testing.assert_array_equal(m["status"][good], a["status"])
+    np.testing.assert_array_equal(m["steps"][good], a["steps"])
+    # every ray, finite or not, stops at the last save
+    assert m["steps"].max() <= sched.last_step
