@@ -342,3 +342,33 @@ def test_nonfinite_rays_are_flagged_and_leave_the_others_unchanged(precision):
     np.testing.assert_array_equal(m["steps"][good], a["steps"])
     # every ray, finite or not, stops at the last save
     assert m["steps"].max() <= sched.last_step
+
+
+@pytest.mark.parametrize("shape", [(2, 2, 2), (2, 3, 5), (5, 2, 3)])
+def test_smallest_grids(shape):
+    """Grids of two points on some axes (one cell; the smallest the ABI
+    takes): the cell index clamps to 0, the one-sided gradients of the pack
+    are the only ones, and no interior run fits. FP64 and FP32 against the
+    oracle with the module's tolerances."""
+    rng = np.random.RandomState(sum(shape))
+    ne = (1e25 * (1.0 + 0.3 * rng.rand(*shape))).astype(np.float32)
+    h = tuple(L / (n - 1) for n in shape)
+    origin = (-L / 2,) * 3
+    omega = 2 * np.pi * C / 532e-9
+    rays = workloads.gaussian_beam(500, waist=1.5e-3, L=L, seed=3).numpy()
+    sched = runtime.schedule_times(np.linspace(0.0, L, 3), h)
+    kw = dict(inv_brems=True, Te=20.0, Z=1.0)
+    o = run_oracle(ne, rays, origin, h, omega, sched, **kw)
+    k64 = run_kernel(ne, rays, origin, h, omega, sched, precision="f64", **kw)
+    assert position_error(k64["state"], o["state"], L) < 1e-10
+    assert direction_error(k64["state"], o["state"]) < 1e-10
+    np.testing.assert_allclose(k64["phase"], o["phase"], rtol=0, atol=1e-10 * np.abs(o["phase"]).max())
+    np.testing.assert_allclose(k64["amp"], o["amp"], rtol=0, atol=1e-12)
+    np.testing.assert_array_equal(k64["steps"], o["steps"])
+    k32 = run_kernel(ne, rays, origin, h, omega, sched, precision="f32", **kw)
+    assert position_error(k32["state"], o["state"], L) < 1e-6
+    assert direction_error(k32["state"], o["state"]) < 1e-6
+    far = (np.abs(o["state"][-1][0]) <= L / 2) & (np.abs(o["state"][-1][1]) <= L / 2)
+    assert far.mean() > 0.9
+    assert np.abs(k32["phase"] - o["phase"])[:, far].max() <= 1e-6 * np.abs(o["phase"]).max()
+    assert np.abs(k32["amp"].astype(np.float64) - o["amp"])[:, far].max() < 1e-6
