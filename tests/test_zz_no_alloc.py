@@ -96,3 +96,19 @@ def test_noalloc_rejects_too_many_rays():
     rc = lib.sloth_trace_f32_noalloc(g, None, _capi.SlothTraceParams(), None, _capi.SLOTH_NOALLOC_MAX_RAYS + 1,
                                      _capi.SlothTraceOutputs(), None)
     assert rc == _capi.SLOTH_ERR_TOO_LARGE
+
+
+def test_noalloc_at_its_maximum_size():
+    """Exactly SLOTH_NOALLOC_MAX_RAYS rays: the keys, permutation and sorted
+    keys fill the fixed scratch to its last byte, and the results equal the
+    workspace entry point's."""
+    n_max = _capi.SLOTH_NOALLOC_MAX_RAYS    # a scratch too small would fail with WORKSPACE_TOO_SMALL
+    dev = torch.device("cuda", 0)
+    n = 32
+    h = L / (n - 1)
+    omega = physics.omega_of(532e-9)
+    ne = workloads.kolmogorov_box(n, L=L, seed=31, device=dev)
+    grid = runtime.pack_grid(ne, (-L / 2,) * 3, (h,) * 3, omega, precision="f32")
+    rays = workloads.gaussian_beam(n_max, waist=2e-3, L=L, seed=32, device=dev).contiguous()
+    sched = runtime.schedule_times(np.linspace(0.0, L, 2), (h, h, h))
+    _compare(_trace("noalloc", grid, rays, sched), _trace("workspace", grid, rays, sched))
