@@ -130,6 +130,10 @@ class RayServer:
                    "sloth_server_submit")
         job = Job(jid.value, n_rays, sched.n_saves, bool(inv_brems),
                   arrival=time.perf_counter() if arrival is None else arrival, keep=[ne, rays])
+        if n_rays == 0:
+            # the server finishes a job without rays at once (FETCHED); its
+            # results are empty arrays of the usual shapes
+            job.out = self._host_outputs(job)
         self.jobs[job.id] = job
         return job
 
@@ -149,16 +153,23 @@ class RayServer:
             job.keep = []
         return st.value
 
+    @staticmethod
+    def _host_outputs(job: Job) -> dict:
+        """Host buffers for a job's results (pinned when there is anything to copy)."""
+        S, N = job.n_saves, job.n
+        pin = N > 0
+        o = {"jones": torch.empty((S, 4, N), dtype=torch.float32, pin_memory=pin),
+             "phase": torch.empty((S, N), dtype=torch.float64, pin_memory=pin),
+             "status": torch.empty(N, dtype=torch.uint8, pin_memory=pin),
+             "steps": torch.empty(N, dtype=torch.int32, pin_memory=pin),
+             "total_steps": torch.zeros(1, dtype=torch.int64, pin_memory=pin)}
+        if job.inv_brems:
+            o["amp"] = torch.empty((S, N), dtype=torch.float32, pin_memory=pin)
+        return o
+
     def fetch(self, job: Job):
         """Start downloading a DONE job's results into pinned host buffers."""
-        S, N = job.n_saves, job.n
-        o = {"jones": torch.empty((S, 4, N), dtype=torch.float32, pin_memory=True),
-             "phase": torch.empty((S, N), dtype=torch.float64, pin_memory=True),
-             "status": torch.empty(N, dtype=torch.uint8, pin_memory=True),
-             "steps": torch.empty(N, dtype=torch.int32, pin_memory=True),
-             "total_steps": torch.zeros(1, dtype=torch.int64, pin_memory=True)}
-        if job.inv_brems:
-            o["amp"] = torch.empty((S, N), dtype=torch.float32, pin_memory=True)
+        o = self._host_outputs(job)
         dst = capi.SlothTraceOutputs()
         for k, t in o.items():
             setattr(dst, k, t.data_ptr())

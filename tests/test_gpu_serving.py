@@ -138,3 +138,24 @@ def test_dense_job_in_the_mix_with_fast_path_jobs():
     direct = runtime.trace(g, rays_d, sched, project=True, plane=L / 2, inv_brems=True, Te=20.0, Z=1.0)
     torch.cuda.synchronize()
     _same(outs[-1], {k: v.cpu() for k, v in direct.items()})
+
+
+def test_job_without_rays_in_the_mix():
+    """A job of zero rays finishes at once with empty results of the usual
+    shapes; the job submitted beside it is unaffected."""
+    specs = [("kolmogorov", 32, 3000, 7)]
+    fields = _fields(specs)
+    with serving.RayServer(1 << 30) as srv:
+        kind, n, nr, seed = specs[0]
+        job, rays = _submit(srv, fields, kind, n, nr, seed)
+        h = L / (n - 1)
+        key = serving.grid_key(kind, n, 0)
+        empty = srv.submit(key, fields[key], (-L / 2,) * 3, (h,) * 3, (n,) * 3,
+                           torch.empty((6, 0), dtype=torch.float32, device="cuda"), lwl=LWL,
+                           detector_plane=L / 2, inv_brems=True, Te=20.0, Z=1.0, n_saves=3)
+        res = srv.run_until_done([job, empty])
+        assert srv.state(empty) == _capi.SLOTH_JOB_FETCHED
+    e = res[empty.id]
+    assert e["jones"].shape == (3, 4, 0) and e["phase"].shape == (3, 0) and e["amp"].shape == (3, 0)
+    assert e["status"].shape == (0,) and int(e["total_steps"][0]) == 0
+    _same(res[job.id], _direct(fields, kind, n, rays))
