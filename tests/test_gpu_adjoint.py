@@ -223,3 +223,15 @@ def test_process_group_of_one_matches_the_local_model():
         assert _rel(x.grad.cpu(), grad) < 1e-12
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_no_rays_give_a_zero_image_and_gradient(precision):
+    """Zero rays: the image is all zeros, and so is d loss / d ne, of the
+    grid's shape, for any target."""
+    h, _, ne1, _, spec = _small()
+    rays = torch.zeros((6, 0), dtype=torch.float64)
+    target = torch.rand(tuple(spec.n_px), dtype=torch.float64)
+    img, g = _kernel(ne1, rays, h, spec, precision, target)
+    assert img.shape == tuple(spec.n_px) and not img.any()
+    assert g.shape == ne1.shape and not g.any()
