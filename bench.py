@@ -245,7 +245,8 @@ def run_serving(args):
            "host_loop_max_ms": live["host_loop_max_ms"],
            "saturated_gpu_busy_frac": sat["stats"]["gpu_busy_ms"] / max(sat["stats"]["gpu_span_ms"], 1e-9),
            "budget_bytes": live["stats"]["budget_bytes"],
-           "stream": "2000 requests, Poisson 200/s, grids {64,128,192,256,384}^3 sinusoid|Kolmogorov, "
+           "stream": f"{args.serving_requests} requests, Poisson 200/s, grids {{64,128,192,256,384}}^3 "
+                     "sinusoid|Kolmogorov, "
                      "lognormal rays median 2e5 sigma 1 in [1e4, 4e6], 120 GB budget; latency = arrival to "
                      "results in pinned host memory; the saturated run (every request queued at once) runs "
                      "first and warms the host allocators"}
