@@ -43,23 +43,30 @@ def test_ctypes_structs_match_the_c_header(tmp_path):
     assert got == expected
 
 
-def test_integration_stub_structs_match_the_binding():
-    """The ctypes stub that INTEGRATION.md shows a SLOTH maintainer declares
-    the same struct layouts as the binding (its class definitions run here;
-    the library loading lines do not)."""
-    import re
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    blocks = re.findall(r"```python\n(.*?)```", text, flags=re.S)
-    stub = next(b for b in blocks if "class TraceParams(Structure)" in b)
-    import ast
-    tree = ast.parse(stub)
-    keep = [n for n in tree.body if isinstance(n, (ast.Import, ast.ImportFrom, ast.ClassDef))]
-    ns = {}
-    exec(compile(ast.Module(body=keep, type_ignores=[]), "INTEGRATION.md", "exec"), ns)
+def _stub():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("sloth_b200_ctypes", os.path.join(ROOT, "include", "sloth_b200_ctypes.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_reference_side_stub_structs_match_the_binding():
+    """The ctypes stub a SLOTH maintainer adds (include/sloth_b200_ctypes.py)
+    declares the same struct layouts as the package's binding."""
+    ns = _stub()
     for stub_name, name in (("GridDesc", "SlothGridDesc"), ("TraceParams", "SlothTraceParams"),
                             ("TraceOutputs", "SlothTraceOutputs")):
-        a, b = ns[stub_name], getattr(_capi, name)
+        a, b = getattr(ns, stub_name), getattr(_capi, name)
         assert _capi.ctypes.sizeof(a) == _capi.ctypes.sizeof(b), stub_name
         assert [f for f, _ in a._fields_] == [f for f, _ in b._fields_], stub_name
         for f, _ in a._fields_:
             assert getattr(a, f).offset == getattr(b, f).offset, (stub_name, f)
+
+
+def test_reference_side_stub_loads_the_library():
+    """The stub opens the built library and finds every entry point it declares
+    (no compute call: no GPU is needed)."""
+    lib = _stub().load(_capi.LIB_PATH)
+    assert lib.sloth_trace_workspace_bytes(1000) > 0
+    assert lib.sloth_strerror(0)
