@@ -1,13 +1,12 @@
 // K2 (FP32 split) and K3 (FP64 port) tracer entry points: one trace of one
 // ray set through one grid (the device code is in tracer.cuh).
 #include <algorithm>
-#include <mutex>
 
 #include "tracer.cuh"
 
 namespace sloth {
 
-template <class P, int IB, bool SMALLX, int FAST>
+template <class P, int IB, bool SMALLX, int FAST, int INTEG>
 __global__ void __launch_bounds__(kThreads, SLOTH_TRACE_MIN_BLOCKS)
 trace_kernel(const __grid_constant__ TraceArgs a) {
     __shared__ unsigned s_key[kTile];
@@ -39,13 +38,13 @@ trace_kernel(const __grid_constant__ TraceArgs a) {
             start = (long long)a.n_big * kTile + (long long)(tile - a.n_big) * kSmallTile;
             cnt = (int)min((long long)kSmallTile, a.n - start);
         }
-        trace_tile<P, IB, SMALLX, FAST>(a, start, cnt, s_key, s_id, &s_head, cc, my_steps);
+        trace_tile<P, IB, SMALLX, FAST, INTEG>(a, start, cnt, s_key, s_id, &s_head, cc, my_steps);
     }
     // one atomic per CTA for the ray-step total
     block_add(my_steps, &s_steps, a.total_steps);
 }
 
-template <class P, int IB, bool SMALLX, int FAST>
+template <class P, int IB, bool SMALLX, int FAST, int INTEG>
 static int launch_trace_k(const TraceArgs& ta, int sms, cudaStream_t s) {
     static int cached[64] = {0};
     int dev = 0;
@@ -53,7 +52,7 @@ static int launch_trace_k(const TraceArgs& ta, int sms, cudaStream_t s) {
     if (e != cudaSuccess) return cuda_status(e);
     int per_sm = (dev >= 0 && dev < 64) ? cached[dev] : 0;
     if (per_sm <= 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel<P, IB, SMALLX, FAST>, kThreads, 0) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel<P, IB, SMALLX, FAST, INTEG>, kThreads, 0) !=
                 cudaSuccess || per_sm < 1)
             per_sm = 1;
         if (dev >= 0 && dev < 64) cached[dev] = per_sm;
@@ -66,16 +65,22 @@ static int launch_trace_k(const TraceArgs& ta, int sms, cudaStream_t s) {
     const long long rest = ta.n - (long long)t.n_big * kTile;
     t.n_tiles = t.n_big + (int)((rest + kSmallTile - 1) / kSmallTile);
     if (blocks > t.n_tiles) blocks = t.n_tiles;
-    trace_kernel<P, IB, SMALLX, FAST><<<(int)blocks, kThreads, 0, s>>>(t);
+    trace_kernel<P, IB, SMALLX, FAST, INTEG><<<(int)blocks, kThreads, 0, s>>>(t);
     note_launch();
     return cuda_status(cudaGetLastError());
 }
 
+template <class P, int IB, bool SMALLX, int INTEG>
+static int launch_trace_i(const TraceArgs& ta, int sms, cudaStream_t s, int fast) {
+    return fast == 1 ? launch_trace_k<P, IB, SMALLX, 1, INTEG>(ta, sms, s)
+         : fast == 2 ? launch_trace_k<P, IB, SMALLX, 2, INTEG>(ta, sms, s)
+                     : launch_trace_k<P, IB, SMALLX, 0, INTEG>(ta, sms, s);
+}
+
 template <class P, int IB, bool SMALLX>
-static int launch_trace(const TraceArgs& ta, int sms, cudaStream_t s, int fast) {
-    return fast == 1 ? launch_trace_k<P, IB, SMALLX, 1>(ta, sms, s)
-         : fast == 2 ? launch_trace_k<P, IB, SMALLX, 2>(ta, sms, s)
-                     : launch_trace_k<P, IB, SMALLX, 0>(ta, sms, s);
+static int launch_trace(const TraceArgs& ta, int sms, cudaStream_t s, int fast, int integ) {
+    return integ == INTEG_RK4 ? launch_trace_i<P, IB, SMALLX, INTEG_RK4>(ta, sms, s, fast)
+                              : launch_trace_i<P, IB, SMALLX, INTEG_RKN>(ta, sms, s, fast);
 }
 
 template <class P>
@@ -135,13 +140,15 @@ static int trace_impl(const SlothGridDesc* g, const void* grid, const SlothTrace
         e = cudaEventRecord((cudaEvent_t)out->trace_event_begin, s);
         if (e != cudaSuccess) return cuda_status(e);
     }
+    const int integ = p->integrator;
     if (ib == IB_OFF)
-        rc = smallx ? launch_trace<P, IB_OFF, true>(ta, sms, s, fast) : launch_trace<P, IB_OFF, false>(ta, sms, s, fast);
+        rc = smallx ? launch_trace<P, IB_OFF, true>(ta, sms, s, fast, integ)
+                    : launch_trace<P, IB_OFF, false>(ta, sms, s, fast, integ);
     else if (ib == IB_SUBCRITICAL)
-        rc = smallx ? launch_trace<P, IB_SUBCRITICAL, true>(ta, sms, s, fast)
-                    : launch_trace<P, IB_SUBCRITICAL, false>(ta, sms, s, fast);
+        rc = smallx ? launch_trace<P, IB_SUBCRITICAL, true>(ta, sms, s, fast, integ)
+                    : launch_trace<P, IB_SUBCRITICAL, false>(ta, sms, s, fast, integ);
     else
-        rc = launch_trace<P, IB_GENERAL, false>(ta, sms, s, fast);
+        rc = launch_trace<P, IB_GENERAL, false>(ta, sms, s, fast, integ);
     if (rc) return rc;
     if (out->trace_event_end) {
         e = cudaEventRecord((cudaEvent_t)out->trace_event_end, s);
@@ -155,8 +162,10 @@ static int trace_impl(const SlothGridDesc* g, const void* grid, const SlothTrace
 // bucket histogram, keys, permutation) lives in one file-scope device array
 // sized for SLOTH_NOALLOC_MAX_RAYS rays, so the caller passes only inputs and
 // outputs and nothing here allocates. Host code cannot use the array's name
-// as a device address; each device's address is looked up once, on that
-// device's first call, with cudaGetSymbolAddress. All calls share the array,
+// as a device address; every call looks the current device's address up with
+// cudaGetSymbolAddress (the first call on a device also loads the library's
+// device code there). A cached address would dangle after cudaDeviceReset,
+// which reloads the device code at a new address. All calls share the array,
 // which keeps the previous call's contents (the tracer zeroes the parts that
 // must start at zero), so calls that overlap on the GPU race.
 // ---------------------------------------------------------------------------
@@ -165,22 +174,12 @@ static_assert(kNoAllocScratchBytes % 256 == 0, "scratch sections must stay 256-b
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-static std::mutex g_noalloc_mutex;
-static void* g_noalloc_addr[64] = {nullptr};
-
 static int noalloc_scratch(void** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* addr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_status(e);
-    if (dev < 0 || dev >= 64) return SLOTH_ERR_UNSUPPORTED_DEVICE;
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (g_noalloc_addr[dev] == nullptr) {
-        void* addr = nullptr;
-        e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_status(e);
-        g_noalloc_addr[dev] = addr;
-    }
-    *out = g_noalloc_addr[dev];
+    if (addr == nullptr || ((uintptr_t)addr & 255u) != 0) return SLOTH_ERR_MISALIGNED;
+    *out = addr;
     return SLOTH_OK;
 }
 

@@ -3,10 +3,10 @@
 It serves callers that cannot allocate device memory (e.g. an XLA FFI
 handler inside a JAX program, where XLA owns the device memory), so its
 scratch lives in a fixed array inside the library. Two calls in a row, of
-different sizes and inputs, must each give what sloth_trace_f32 (with a
-caller workspace) gives, within the FP32 tolerances of the parity tests:
-positions 1e-6 of the box, angles 1e-6 rad, phase 1e-6 relative, amplitude
-1e-6. The file is named to be collected last.
+different sizes and inputs, must each give bitwise what sloth_trace_f32
+(with a caller workspace) gives: both run the same tracer on the same
+inputs, and each ray's arithmetic does not depend on the scratch layout.
+The file is named to be collected last.
 """
 import math
 
@@ -61,15 +61,15 @@ def _trace(entry, grid, rays, sched):
     return {k: v.cpu() for k, v in o.items()}
 
 
+def _bits(t):
+    """The tensor's bit patterns (NaN compares equal to the same NaN)."""
+    return t.view({torch.float32: torch.int32, torch.float64: torch.int64}.get(t.dtype, t.dtype))
+
+
 def _compare(a, b):
-    ja, jb = a["jones"].double(), b["jones"].double()
-    assert (ja[:, [0, 2]] - jb[:, [0, 2]]).abs().max().item() <= 1e-6 * L
-    assert (ja[:, [1, 3]] - jb[:, [1, 3]]).abs().max().item() <= 1e-6
-    ph = max(b["phase"].abs().max().item(), 1e-30)
-    assert (a["phase"] - b["phase"]).abs().max().item() <= 1e-6 * ph
-    assert (a["amp"].double() - b["amp"].double()).abs().max().item() <= 1e-6
-    assert torch.equal(a["status"], b["status"]) and torch.equal(a["steps"], b["steps"])
-    assert int(a["total_steps"][0]) == int(b["total_steps"][0]) == int(b["steps"].long().sum())
+    for k in ("jones", "phase", "amp", "status", "steps", "total_steps"):
+        assert torch.equal(_bits(a[k]), _bits(b[k])), k
+    assert int(a["total_steps"][0]) == int(b["steps"].long().sum())
 
 
 def test_noalloc_matches_workspace_entry_point_twice():
