@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define SLOTH_ABI_VERSION 2
+#define SLOTH_ABI_VERSION 3
 
 /* ---- return codes ------------------------------------------------------ */
 #define SLOTH_OK                        0
@@ -57,8 +57,13 @@ typedef struct SlothGridDesc {
     double  spacing[3];  /* uniform spacing per axis (m), > 0                 */
 } SlothGridDesc;
 
+/* Integration methods of the tracers (SlothTraceParams::integrator). */
+#define SLOTH_INTEGRATOR_RKN 0   /* Nystrom's 4th-order Runge-Kutta-Nystrom: 3 field samples per step */
+#define SLOTH_INTEGRATOR_RK4 1   /* classical RK4 of the first-order system: 4 field samples per step */
+
 /* Fixed-step schedule and physics of one trace (fourth-order Runge-Kutta-
- * Nystrom steps: three field samples per step).
+ * Nystrom steps, three field samples per step, or classical RK4 steps, four
+ * samples; `integrator`).
  * All steps have the same length dtau (tau = c*t, metres). Save j (0-based)
  * is taken after step first_save + j*save_every; the trace ends at the last
  * save. Rays that have left the grid for good are advanced to later saves by
@@ -92,6 +97,9 @@ typedef struct SlothTraceParams {
                                  (bitwise the same results in FP32, within 1e-12
                                  relative in FP64; fewer instructions). A value above
                                  the true minimum is an error of the caller. */
+    int32_t integrator;       /* SLOTH_INTEGRATOR_RKN (0, default) or SLOTH_INTEGRATOR_RK4;
+                                 the request server takes RKN steps only          */
+    int32_t reserved;         /* must be 0                                          */
 } SlothTraceParams;
 
 #define SLOTH_MAX_SAVES 4096
@@ -180,7 +188,8 @@ int sloth_trace_f64(const SlothGridDesc* g, const void* grid, const SlothTracePa
  * to two iterations in flight. Results of a job do not depend on the other
  * jobs in its iterations. Lifecycle of a job:
  *   PENDING -> RUNNING (admitted) -> DONE -> fetch -> FETCHING -> FETCHED
- * (memory released), or a negative SLOTH_ERR_* state if admission failed.
+ * (memory released), or a negative SLOTH_ERR_* state if admission failed,
+ * or CANCELLED (sloth_server_cancel) from PENDING, RUNNING or DONE.
  * The caller keeps `ne` (needed until the job is admitted, and only if the
  * grid key is not resident) and `rays` valid until the job leaves PENDING.
  * A handle may be used from several host threads (calls are serialised). */
@@ -201,6 +210,8 @@ typedef struct SlothServerStats {
     long long iterations, tiles, kernel_launches;
     double    gpu_busy_ms;   /* time some iteration was running on the GPU (union)  */
     double    gpu_span_ms;   /* first iteration start to last finished iteration end */
+    long long jobs_cancelled;
+    long long cancelled_pending_free;   /* cancelled jobs whose memory waits for in-flight iterations */
 } SlothServerStats;
 
 #define SLOTH_JOB_PENDING  0
@@ -208,6 +219,7 @@ typedef struct SlothServerStats {
 #define SLOTH_JOB_DONE     2
 #define SLOTH_JOB_FETCHING 3
 #define SLOTH_JOB_FETCHED  4
+#define SLOTH_JOB_CANCELLED 5
 
 int sloth_server_create(const SlothServerConfig* cfg, SlothServer** out);
 int sloth_server_destroy(SlothServer* s);
@@ -226,8 +238,23 @@ int sloth_server_job_state(SlothServer* s, int job_id, int* state);
  * pointers; NULL skips; element types as for sloth_trace_f32, no state);
  * the job's memory is released once the copy has finished (FETCHED). */
 int sloth_server_fetch(SlothServer* s, int job_id, const SlothTraceOutputs* dst);
-/* Forgets a DONE or FETCHED job (a DONE job's memory is released unread). */
+/* Forgets a DONE, FETCHED or CANCELLED job (a DONE job's memory is released
+ * unread). */
 int sloth_server_release(SlothServer* s, int job_id);
+/* Cancels a job; never blocks on the GPU. A PENDING job leaves the queue; a
+ * RUNNING job gets no further tiles, and its memory and table slot are
+ * released once the iterations already holding its tiles have finished on
+ * the GPU (stats.cancelled_pending_free counts such jobs); a DONE job's
+ * memory is released unread. The job's state becomes CANCELLED at once.
+ * CANCELLED, FETCHED and failed jobs are left as they are (SLOTH_OK);
+ * a FETCHING job returns SLOTH_ERR_BUSY. No counterpart in the reference. */
+int sloth_server_cancel(SlothServer* s, int job_id);
+/* Fault injection for tests of the create path: the next
+ * sloth_server_create reports the `nth` (1-based) of its device or pinned
+ * host allocations as failed (cudaErrorMemoryAllocation) without making it,
+ * releases what it had allocated and returns SLOTH_ERR_OUT_OF_MEMORY.
+ * One-shot; 0 disarms. Returns the number of allocations create makes. */
+int sloth_server_inject_alloc_failure(int nth);
 int sloth_server_stats(SlothServer* s, SlothServerStats* st);
 /* Waits for all work the server has launched. */
 int sloth_server_sync(SlothServer* s);
@@ -245,8 +272,11 @@ int sloth_server_sync(SlothServer* s);
  *   - n <= SLOTH_NOALLOC_MAX_RAYS, else SLOTH_ERR_TOO_LARGE;
  *   - the array (about 13.6 MB) is held on every GPU that loads the library
  *     until the process exits;
- *   - the first call on each device looks up the array's device address with
- *     cudaGetSymbolAddress; make that first call before any stream capture;
+ *   - every call looks up the array's device address on the current device
+ *     with cudaGetSymbolAddress, so the address stays right after
+ *     cudaDeviceReset; the first call on each device also loads the
+ *     library's device code there: make that first call before any stream
+ *     capture;
  *   - every call shares the array, so calls that overlap on the GPU (other
  *     streams, other host threads) race: serialise them.
  * Results equal sloth_trace_f32's for the same inputs. */

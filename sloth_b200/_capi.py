@@ -61,7 +61,8 @@ class SlothTraceParams(Structure):
                 ("first_save", c_int32), ("save_every", c_int32), ("n_saves", c_int32),
                 ("probing_axis", c_int32), ("project_to_plane", c_int32), ("inv_brems", c_int32),
                 ("plane", c_double), ("kappa_q2", c_double), ("coulomb_log_w", c_double),
-                ("ope_ratio2", c_double), ("q_max", c_double), ("q_min", c_double)]
+                ("ope_ratio2", c_double), ("q_max", c_double), ("q_min", c_double),
+                ("integrator", c_int32), ("reserved", c_int32)]
 
 
 class SlothTraceOutputs(Structure):
@@ -81,7 +82,8 @@ class SlothServerStats(Structure):
                 ("jobs_submitted", ctypes.c_longlong), ("jobs_admitted", ctypes.c_longlong),
                 ("jobs_done", ctypes.c_longlong), ("jobs_failed", ctypes.c_longlong),
                 ("iterations", ctypes.c_longlong), ("tiles", ctypes.c_longlong),
-                ("kernel_launches", ctypes.c_longlong), ("gpu_busy_ms", c_double), ("gpu_span_ms", c_double)]
+                ("kernel_launches", ctypes.c_longlong), ("gpu_busy_ms", c_double), ("gpu_span_ms", c_double),
+                ("jobs_cancelled", ctypes.c_longlong), ("cancelled_pending_free", ctypes.c_longlong)]
 
 
 class SlothOptic(Structure):
@@ -116,6 +118,8 @@ class SlothImageParams(Structure):
 
 
 SLOTH_JOB_PENDING, SLOTH_JOB_RUNNING, SLOTH_JOB_DONE, SLOTH_JOB_FETCHING, SLOTH_JOB_FETCHED = 0, 1, 2, 3, 4
+SLOTH_JOB_CANCELLED = 5
+SLOTH_INTEGRATOR_RKN, SLOTH_INTEGRATOR_RK4 = 0, 1
 
 # name -> (restype, argtypes); every symbol include/sloth_b200.h declares.
 _SIGNATURES = {
@@ -145,6 +149,8 @@ _SIGNATURES = {
     "sloth_server_release": (c_int, [c_void_p, c_int]),
     "sloth_server_stats": (c_int, [c_void_p, POINTER(SlothServerStats)]),
     "sloth_server_sync": (c_int, [c_void_p]),
+    "sloth_server_cancel": (c_int, [c_void_p, c_int]),
+    "sloth_server_inject_alloc_failure": (c_int, [c_int]),
     "sloth_image_workspace_bytes": (c_size_t, [POINTER(SlothImageParams), c_int64]),
     "sloth_image_forward_f32": (c_int, [POINTER(SlothGridDesc), c_void_p, POINTER(SlothImageParams), c_void_p,
                                         c_int64, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),

@@ -24,6 +24,7 @@
 // Each ray is traced by exactly the code of the single-trace kernel
 // (trace_tile in tracer.cuh), so a job's results do not depend on which
 // other jobs share its iterations.
+#include <atomic>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -109,20 +110,7 @@ serve_kernel(const TraceArgs* __restrict__ table, WorkHeader* hdr, const WorkIte
 // ---------------------------------------------------------------------------
 class Arena {
   public:
-    int init(size_t bytes) {
-        bytes = (bytes + 255u) & ~(size_t)255u;
-        cudaError_t e = cudaMalloc(&base_, bytes);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            base_ = nullptr;
-            return cuda_status(e);
-        }
-        size_ = bytes;
-        free_.clear();
-        free_[0] = bytes;
-        used_ = 0;
-        return SLOTH_OK;
-    }
+    int init(size_t bytes, int* alloc_counter);
     void destroy() {
         if (base_) cudaFree(base_);
         base_ = nullptr;
@@ -208,6 +196,15 @@ struct Job {
     cudaEvent_t fetched = nullptr;
 };
 
+// Memory of a cancelled RUNNING job, released once the iterations that
+// hold its tiles have finished.
+struct DeferredFree {
+    size_t off = 0, bytes = 0;
+    int slot = -1;
+    uint64_t grid_key = 0;
+    long long last_iter = -1;
+};
+
 struct IterSlot {
     cudaStream_t stream = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -230,6 +227,7 @@ struct ServerImpl {
     std::unordered_map<int, Job> jobs;
     std::deque<int> pending;
     std::vector<int> admitted;      // jobs holding a slot, in admission order
+    std::vector<DeferredFree> deferred;   // cancelled running jobs' memory
     size_t rr = 0;                  // round-robin cursor into `admitted`
     int next_id = 1;
     unsigned long long clock = 0;
@@ -483,6 +481,18 @@ static void retire(ServerImpl* s) {
             ++i;
         }
     }
+    // cancelled jobs whose tiles have all run
+    for (size_t i = 0; i < s->deferred.size();) {
+        const DeferredFree& d = s->deferred[i];
+        if (d.last_iter <= s->iter_done) {
+            if (d.bytes) s->arena.release(d.off, d.bytes);
+            if (d.slot >= 0) s->free_slots.push_back(d.slot);
+            grid_unref(s, d.grid_key);
+            s->deferred.erase(s->deferred.begin() + i);
+        } else {
+            ++i;
+        }
+    }
     // finished downloads free their memory
     for (auto& kv : s->jobs) {
         Job& j = kv.second;
@@ -549,6 +559,38 @@ static int launch_iteration(ServerImpl* s) {
     return SLOTH_OK;
 }
 
+// Fault injection of sloth_server_create's allocations (tests): the
+// allocation with this 1-based index fails once; 0 is off.
+static std::atomic<int> g_fail_alloc_at{0};
+constexpr int kCreateAllocs = 3 + 2 * 2;   // arena, table, pinned table, and per iteration slot two buffers
+
+static cudaError_t create_alloc(void** p, size_t bytes, bool pinned_host, int* counter) {
+    const int k = ++*counter;
+    int armed = k;
+    if (g_fail_alloc_at.compare_exchange_strong(armed, 0)) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return pinned_host ? cudaMallocHost(p, bytes) : cudaMalloc(p, bytes);
+}
+
+int Arena::init(size_t bytes, int* alloc_counter) {
+    bytes = (bytes + 255u) & ~(size_t)255u;
+    void* p = nullptr;
+    cudaError_t e = create_alloc(&p, bytes, false, alloc_counter);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        base_ = nullptr;
+        return cuda_status(e);
+    }
+    base_ = static_cast<char*>(p);
+    size_ = bytes;
+    free_.clear();
+    free_[0] = bytes;
+    used_ = 0;
+    return SLOTH_OK;
+}
+
 }  // namespace sloth
 
 using sloth::ServerImpl;
@@ -572,14 +614,17 @@ int sloth_server_create(const SlothServerConfig* cfg, SlothServer** out) {
     int rc = sloth::device_sm_count(&s->sms);
     cudaError_t e = cudaGetDevice(&s->device);
     if (!rc && e != cudaSuccess) rc = sloth::cuda_status(e);
-    if (!rc) rc = s->arena.init(cfg->budget_bytes);
+    int allocs = 0;
+    if (!rc) rc = s->arena.init(cfg->budget_bytes, &allocs);
     auto fail = [&](int code) {
         sloth_server_destroy(srv);
         return code;
     };
     if (rc) return fail(rc);
-    if ((e = cudaMalloc(&s->d_table, sizeof(sloth::TraceArgs) * cfg->max_jobs)) != cudaSuccess ||
-        (e = cudaMallocHost(&s->h_table, sizeof(sloth::TraceArgs) * cfg->max_jobs)) != cudaSuccess ||
+    if ((e = sloth::create_alloc(reinterpret_cast<void**>(&s->d_table), sizeof(sloth::TraceArgs) * cfg->max_jobs,
+                                 false, &allocs)) != cudaSuccess ||
+        (e = sloth::create_alloc(reinterpret_cast<void**>(&s->h_table), sizeof(sloth::TraceArgs) * cfg->max_jobs,
+                                 true, &allocs)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&s->admit, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&s->admit_ev, cudaEventDisableTiming)) != cudaSuccess ||
@@ -595,8 +640,8 @@ int sloth_server_create(const SlothServerConfig* cfg, SlothServer** out) {
     for (auto& is : s->it) {
         if ((e = cudaStreamCreateWithFlags(&is.stream, cudaStreamNonBlocking)) != cudaSuccess ||
             (e = cudaEventCreate(&is.done)) != cudaSuccess || (e = cudaEventCreate(&is.start)) != cudaSuccess ||
-            (e = cudaMallocHost(&is.h_buf, wbytes)) != cudaSuccess ||
-            (e = cudaMalloc(&is.d_buf, wbytes)) != cudaSuccess)
+            (e = sloth::create_alloc(reinterpret_cast<void**>(&is.h_buf), wbytes, true, &allocs)) != cudaSuccess ||
+            (e = sloth::create_alloc(reinterpret_cast<void**>(&is.d_buf), wbytes, false, &allocs)) != cudaSuccess)
             return fail(sloth::cuda_status(e));
         memset(is.h_buf, 0, wbytes);
         if ((rc = sloth::graph_build(s, is, blocks)) != SLOTH_OK) return fail(rc);
@@ -641,6 +686,7 @@ int sloth_server_submit(SlothServer* srv, uint64_t grid_key, const SlothGridDesc
     if (!srv || !p || !job_id) return SLOTH_ERR_NULL_POINTER;
     int rc = sloth::check_trace_params(g, p, n);
     if (rc) return rc;
+    if (p->integrator != SLOTH_INTEGRATOR_RKN) return SLOTH_ERR_INVALID_ARGUMENT;   // the serving kernels take RKN steps
     if (n > 0 && !rays) return SLOTH_ERR_NULL_POINTER;
     ServerImpl* s = &srv->impl;
     std::lock_guard<std::mutex> lock(s->mu);
@@ -746,12 +792,67 @@ int sloth_server_release(SlothServer* srv, int job_id) {
     return SLOTH_OK;
 }
 
+int sloth_server_cancel(SlothServer* srv, int job_id) {
+    if (!srv) return SLOTH_ERR_NULL_POINTER;
+    ServerImpl* s = &srv->impl;
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return SLOTH_ERR_NOT_FOUND;
+    sloth::Job& j = it->second;
+    switch (j.state) {
+        case sloth::JOB_PENDING:
+            for (auto q = s->pending.begin(); q != s->pending.end(); ++q)
+                if (*q == job_id) {
+                    s->pending.erase(q);
+                    break;
+                }
+            break;
+        case sloth::JOB_ADMITTED: {
+            // no further tiles; the memory waits for the iterations that hold
+            // the tiles already handed out (last_iter), which may still run
+            for (size_t i = 0; i < s->admitted.size(); ++i)
+                if (s->admitted[i] == job_id) {
+                    s->admitted.erase(s->admitted.begin() + i);
+                    if (s->rr > i) --s->rr;
+                    break;
+                }
+            sloth::DeferredFree d;
+            d.off = j.off;
+            d.bytes = j.bytes;
+            d.slot = j.slot;
+            d.grid_key = j.grid_key;
+            d.last_iter = j.last_iter;
+            s->deferred.push_back(d);
+            j.bytes = 0;
+            j.slot = -1;
+            j.tiles_total = j.tiles_assigned;
+            break;
+        }
+        case sloth::JOB_DONE:
+            sloth::free_job_memory(s, j);
+            break;
+        case sloth::JOB_FETCHING:
+            return SLOTH_ERR_BUSY;
+        default:
+            return SLOTH_OK;   // FETCHED, CANCELLED or failed: nothing to cancel
+    }
+    j.state = SLOTH_JOB_CANCELLED;
+    ++s->stats.jobs_cancelled;
+    return SLOTH_OK;
+}
+
+int sloth_server_inject_alloc_failure(int nth) {
+    sloth::g_fail_alloc_at.store(nth > 0 ? nth : 0);
+    return sloth::kCreateAllocs;
+}
+
 int sloth_server_stats(SlothServer* srv, SlothServerStats* st) {
     if (!srv || !st) return SLOTH_ERR_NULL_POINTER;
     ServerImpl* s = &srv->impl;
     std::lock_guard<std::mutex> lock(s->mu);
     s->stats.arena_used = s->arena.used();
     s->stats.grids_resident = (long long)s->grids.size();
+    s->stats.cancelled_pending_free = (long long)s->deferred.size();
     *st = s->stats;
     return SLOTH_OK;
 }

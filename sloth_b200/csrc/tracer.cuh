@@ -61,6 +61,11 @@ constexpr double kSmallX = 0.05;         // bound on (omega_pe/omega)^2 for the 
 // Inverse-bremsstrahlung modes of the tracer.
 enum { IB_OFF = 0, IB_SUBCRITICAL = 1, IB_GENERAL = 2 };
 
+// Integration methods (SlothTraceParams::integrator): Nystrom's fourth-order
+// Runge-Kutta-Nystrom step (3 field samples) or the classical RK4 step of
+// the first-order system (4 samples).
+enum { INTEG_RKN = SLOTH_INTEGRATOR_RKN, INTEG_RK4 = SLOTH_INTEGRATOR_RK4 };
+
 // How a step samples its stage points: PLAIN tests each point against the
 // grid (fill 0 outside); CLAMP moves it into the grid first (steps at a
 // face); INTERIOR skips the test, for steps whose stage points are known to
@@ -720,11 +725,211 @@ __device__ __forceinline__ void rkn_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
     if constexpr (IB != IB_OFF) r.tau.add(mphi(kq));
 }
 
+// One classical RK4 step of the first-order system (p, w)' = (w, A(p)) of
+// length phi, four samples of the field (the integrator the workload
+// descriptions name; INTEG_RK4):
+//   stage points p, p + phi*w/2, p + phi*w2/2, p + phi*w3
+//   with w2 = w + phi*A1/2, w3 = w + phi*A2/2;
+//   p' = p + phi*w + phi^2 (A1 + A2 + A3)/6,  w' = w + phi (A1 + 2A2 + 2A3 + A4)/6,
+// and the phase and depth take RK4's weights (1, 2, 2, 1)/6 on the stages.
+// The stage points lie within phi^2 |A|/4 and phi^2 |A|/2 of the segment
+// from p to p + phi*w, as the RKN step's do, so the interior-sampling bound
+// kInteriorAccel and the interior-run envelope hold for both methods.
+template <class P, int IB, bool SMALLX, int MODE, class Cache>
+__device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
+    using R = typename P::R;
+    const R two = R(2);
+    const R hphi = R(0.5) * phi, phi6 = phi * R(1.0 / 6.0), phi2_6 = phi * phi6;
+    const R S0 = arg_S<R>(a, 0), S1 = arg_S<R>(a, 1), S2 = arg_S<R>(a, 2);
+    const R ope2 = arg_ope2<R>(a);
+    R ph[3], pl[3], we[3], sA[3], sW[3], w3[3], st[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        ph[x] = r.p[x].hi();
+        pl[x] = r.p[x].lo();
+        we[x] = r.w[x].val();
+    }
+    Sample<P> s;
+    // FP32 with the series form of n - 1 evaluates it for stages (1, 2) and
+    // (3, 4) as pairs
+    constexpr bool kPairPhase = SMALLX && sizeof(R) == 4;
+    // stage 1 at p
+    sample_c<P, IB, MODE>(a, ph, pl, s, cc);
+    R g, q1 = R(0), q3 = R(0);
+    if constexpr (kPairPhase) {
+        q1 = s.q;
+        g = R(0);
+    } else {
+        g = nm1<P, SMALLX>(ope2 * s.q);
+    }
+    R kq = s.k;
+    sA[0] = S0 * s.g0; sA[1] = S1 * s.g1; sA[2] = S2 * s.g2;
+    // stage 2 at p + phi*w/2
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        sW[x] = sA[x];
+        st[x] = pl[x] + hphi * we[x];
+    }
+    sample_c<P, IB, MODE>(a, ph, st, s, cc);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) st[x] = pl[x] + hphi * (we[x] + hphi * sA[x]);   // p + phi*w2/2
+    {
+        const R A[3] = {S0 * s.g0, S1 * s.g1, S2 * s.g2};
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            w3[x] = we[x] + hphi * A[x];
+            sA[x] += A[x];
+            sW[x] += two * A[x];
+        }
+    }
+    if constexpr (kPairPhase) {
+        const float2 n12 = nm1_series2(__fmul2_rn(make_float2(ope2, ope2), make_float2(q1, s.q)));
+        g = n12.x + two * n12.y;
+    } else {
+        g += two * nm1<P, SMALLX>(ope2 * s.q);
+    }
+    kq += two * s.k;
+    // stage 3 at p + phi*w2/2
+    sample_c<P, IB, MODE>(a, ph, st, s, cc);
+    {
+        const R A[3] = {S0 * s.g0, S1 * s.g1, S2 * s.g2};
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            sA[x] += A[x];
+            sW[x] += two * A[x];
+            st[x] = pl[x] + phi * w3[x];
+        }
+    }
+    if constexpr (kPairPhase) {
+        q3 = s.q;
+    } else {
+        g += two * nm1<P, SMALLX>(ope2 * s.q);
+    }
+    kq += two * s.k;
+    // stage 4 at p + phi*w3
+    sample_c<P, IB, MODE>(a, ph, st, s, cc);
+    sW[0] += S0 * s.g0; sW[1] += S1 * s.g1; sW[2] += S2 * s.g2;
+    if constexpr (kPairPhase) {
+        const float2 n34 = nm1_series2(__fmul2_rn(make_float2(ope2, ope2), make_float2(q3, s.q)));
+        g += two * n34.x + n34.y;
+    } else {
+        g += nm1<P, SMALLX>(ope2 * s.q);
+    }
+    kq += s.k;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        const R dp = phi * r.w[x].hi() + (phi * r.w[x].lo() + phi2_6 * sA[x]);
+        r.p[x].add(dp);
+        r.w[x].add(phi6 * sW[x]);
+    }
+    r.ph += (double)(phi * g);
+    if constexpr (IB != IB_OFF) r.tau.add(phi * kq);
+}
+
+// The RK4 step in the paired FP32 form (y and z components as register
+// pairs), rounded exactly as the scalar form rounds each component.
+template <int IB, bool SMALLX, int MODE, bool UNIT, int NK>
+__device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, CellPolyF2<NK>& cc, float phi) {
+    if constexpr (UNIT) phi = 1.0f;
+    const float hphi = 0.5f * phi, phi6 = phi * (1.0f / 6.0f), phi2_6 = phi * phi6;
+    const float S0 = a.Sf[0];
+    const float2 S12 = make_float2(a.Sf[1], a.Sf[2]);
+    const float ope2 = a.ope2f;
+    const float2 hphi2 = bc2(hphi), two2 = bc2(2.0f);
+    const float phx = r.p[0].s, plx = r.p[0].c, wex = __fadd_rn(r.w[0].s, r.w[0].c);
+    const float2 phyz = make_float2(r.p[1].s, r.p[2].s), plyz = make_float2(r.p[1].c, r.p[2].c);
+    const float2 weyz = __fadd2_rn(make_float2(r.w[1].s, r.w[2].s), make_float2(r.w[1].c, r.w[2].c));
+    constexpr bool kPairPhase = SMALLX;
+    Sample<PolF32> s;
+    // stage 1 at p
+    sample_f2<IB, MODE>(a, phx, plx, phyz, plyz, s, cc);
+    float g = 0.0f, q1 = 0.0f, q3 = 0.0f;
+    if constexpr (kPairPhase) q1 = s.q; else g = nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q));
+    float kq = s.k;
+    float sAx = __fmul_rn(S0, s.g0);
+    float2 sAyz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
+    float sWx = sAx;
+    float2 sWyz = sAyz;
+    // stage 2 at p + phi*w/2
+    float stx = __fmaf_rn(hphi, wex, plx);
+    float2 styz = __ffma2_rn(hphi2, weyz, plyz);
+    sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
+    stx = __fmaf_rn(hphi, __fmaf_rn(hphi, sAx, wex), plx);                 // p + phi*w2/2
+    styz = __ffma2_rn(hphi2, __ffma2_rn(hphi2, sAyz, weyz), plyz);
+    float w3x;
+    float2 w3yz;
+    {
+        const float Ax = __fmul_rn(S0, s.g0);
+        const float2 Ayz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
+        w3x = __fmaf_rn(hphi, Ax, wex);
+        w3yz = __ffma2_rn(hphi2, Ayz, weyz);
+        sAx = __fadd_rn(sAx, Ax);
+        sAyz = __fadd2_rn(sAyz, Ayz);
+        sWx = __fmaf_rn(2.0f, Ax, sWx);
+        sWyz = __ffma2_rn(two2, Ayz, sWyz);
+    }
+    if constexpr (kPairPhase) {
+        const float2 n12 = nm1_series2(__fmul2_rn(bc2(ope2), make_float2(q1, s.q)));
+        g = __fmaf_rn(2.0f, n12.y, n12.x);
+    } else {
+        g = __fmaf_rn(2.0f, nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q)), g);
+    }
+    kq = __fmaf_rn(2.0f, s.k, kq);
+    // stage 3 at p + phi*w2/2
+    sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
+    {
+        const float Ax = __fmul_rn(S0, s.g0);
+        const float2 Ayz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
+        sAx = __fadd_rn(sAx, Ax);
+        sAyz = __fadd2_rn(sAyz, Ayz);
+        sWx = __fmaf_rn(2.0f, Ax, sWx);
+        sWyz = __ffma2_rn(two2, Ayz, sWyz);
+        stx = __fmaf_rn(phi, w3x, plx);
+        styz = __ffma2_rn(bc2(phi), w3yz, plyz);
+    }
+    if constexpr (kPairPhase) q3 = s.q; else g = __fmaf_rn(2.0f, nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q)), g);
+    kq = __fmaf_rn(2.0f, s.k, kq);
+    // stage 4 at p + phi*w3
+    sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
+    sWx = __fmaf_rn(S0, s.g0, sWx);
+    sWyz = __ffma2_rn(S12, make_float2(s.g1, s.g2), sWyz);
+    if constexpr (kPairPhase) {
+        const float2 n34 = nm1_series2(__fmul2_rn(bc2(ope2), make_float2(q3, s.q)));
+        g = __fadd_rn(g, __fmaf_rn(2.0f, n34.x, n34.y));
+    } else {
+        g = __fadd_rn(g, nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q)));
+    }
+    kq = __fadd_rn(kq, s.k);
+    // x: the scalar update
+    r.p[0].add(__fmaf_rn(phi, r.w[0].hi(), __fmaf_rn(phi, r.w[0].lo(), __fmul_rn(phi2_6, sAx))));
+    r.w[0].add(__fmul_rn(phi6, sWx));
+    // y, z: the same update on pairs
+    {
+        const float2 phi2 = bc2(phi);
+        const float2 whi = make_float2(r.w[1].s, r.w[2].s), wlo = make_float2(r.w[1].c, r.w[2].c);
+        const float2 dp = __ffma2_rn(phi2, whi, __ffma2_rn(phi2, wlo, __fmul2_rn(bc2(phi2_6), sAyz)));
+        float2 ps = phyz, pc = plyz;
+        kahan2(ps, pc, dp);
+        r.p[1].s = ps.x; r.p[2].s = ps.y; r.p[1].c = pc.x; r.p[2].c = pc.y;
+        float2 ws = whi, wc = wlo;
+        kahan2(ws, wc, __fmul2_rn(bc2(phi6), sWyz));
+        r.w[1].s = ws.x; r.w[2].s = ws.y; r.w[1].c = wc.x; r.w[2].c = wc.y;
+    }
+    r.ph += (double)__fmul_rn(phi, g);
+    if constexpr (IB != IB_OFF) r.tau.add(__fmul_rn(phi, kq));
+}
+
 // One step: the paired FP32 form with the paired cell cache, the generic form
-// otherwise.
-template <class P, int IB, bool SMALLX, int MODE, bool UNIT = false, class Cache>
+// otherwise; RKN unless INTEG selects RK4.
+template <class P, int IB, bool SMALLX, int MODE, bool UNIT = false, int INTEG = INTEG_RKN, class Cache>
 __device__ __forceinline__ void step_any(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
-    if constexpr (IsPairedCache<Cache>::value && SLOTH_PAIRED_STEP) {
+    if constexpr (INTEG == INTEG_RK4) {
+        if constexpr (IsPairedCache<Cache>::value && SLOTH_PAIRED_STEP) {
+            rk4_step_f2<IB, SMALLX, MODE, UNIT>(a, r, cc, phi);
+        } else {
+            rk4_step<P, IB, SMALLX, MODE>(a, r, cc, phi);
+        }
+    } else if constexpr (IsPairedCache<Cache>::value && SLOTH_PAIRED_STEP) {
         rkn_step_f2<IB, SMALLX, MODE, UNIT>(a, r, cc, phi);
     } else {
         rkn_step<P, IB, SMALLX, MODE>(a, r, cc, phi);
@@ -987,7 +1192,7 @@ __device__ __forceinline__ void tile_sort(unsigned* key, unsigned* id, int size)
 // acceleration bound skip it and sample without the grid test (bound at most
 // kInteriorAccel); 2 they skip the face test but sample with the grid test
 // (any finite bound). Every mode takes the same steps.
-template <class P, int IB, bool SMALLX, int FAST, class Cache>
+template <class P, int IB, bool SMALLX, int FAST, int INTEG = INTEG_RKN, class Cache>
 __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, int cnt, unsigned* s_key,
                                            unsigned* s_id, int* s_head, Cache& cc,
                                            unsigned long long& my_steps) {
@@ -1052,16 +1257,16 @@ __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, 
             if (FAST && kind == 0) {
 #pragma unroll 1
                 for (int e = 0;; ++e) {
-                    step_any<P, IB, SMALLX, FAST == 1 ? SAMPLE_INTERIOR : SAMPLE_PLAIN, true>(a, r, cc,
-                                                                                            typename P::R(1));
+                    step_any<P, IB, SMALLX, FAST == 1 ? SAMPLE_INTERIOR : SAMPLE_PLAIN, true, INTEG>(
+                        a, r, cc, typename P::R(1));
                     if (e == extra) break;
                     ++r.step;
                 }
                 r.run -= extra;
             } else if (kind == 0 || kind == 3) {
-                step_any<P, IB, SMALLX, SAMPLE_PLAIN, true>(a, r, cc, typename P::R(1));
+                step_any<P, IB, SMALLX, SAMPLE_PLAIN, true, INTEG>(a, r, cc, typename P::R(1));
             } else {
-                step_any<P, IB, SMALLX, SAMPLE_CLAMP>(a, r, cc, phi);
+                step_any<P, IB, SMALLX, SAMPLE_CLAMP, false, INTEG>(a, r, cc, phi);
                 if (kind == 2) {
                     r.exited = true;
                     r.lag = 1.0 - (double)phi;
@@ -1376,6 +1581,9 @@ inline int check_trace_params(const SlothGridDesc* g, const SlothTraceParams* p,
     if (p->inv_brems && !(p->kappa_q2 >= 0.0)) return SLOTH_ERR_INVALID_ARGUMENT;
     if (p->project_to_plane && !std::isfinite(p->plane)) return SLOTH_ERR_INVALID_ARGUMENT;
     if (!std::isfinite(p->q_max)) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (p->integrator != SLOTH_INTEGRATOR_RKN && p->integrator != SLOTH_INTEGRATOR_RK4)
+        return SLOTH_ERR_INVALID_ARGUMENT;
+    if (p->reserved != 0) return SLOTH_ERR_INVALID_ARGUMENT;
     return SLOTH_OK;
 }
 

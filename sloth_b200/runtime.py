@@ -181,11 +181,22 @@ def _workspace(n: int, device) -> torch.Tensor:
     return t
 
 
+def integrator_code(integrator: str) -> int:
+    """SLOTH_INTEGRATOR_* of 'rkn' or 'rk4'."""
+    codes = {"rkn": capi.SLOTH_INTEGRATOR_RKN, "rk4": capi.SLOTH_INTEGRATOR_RK4}
+    if integrator not in codes:
+        raise ValueError(f"integrator must be 'rkn' or 'rk4', not {integrator!r}")
+    return codes[integrator]
+
+
 def trace(grid: DeviceGrid, rays: torch.Tensor, sched: Schedule, *, axis=2, project=False, plane=0.0,
           inv_brems=False, Te=None, Z=None, want_state=False, want_phase=True, want_amp=None,
           want_status=True, want_steps=True, stream=None, workspace: Optional[torch.Tensor] = None,
-          outputs: Optional[dict] = None, events=None) -> dict:
+          outputs: Optional[dict] = None, events=None, integrator: str = "rkn") -> dict:
     """K2/K3: trace rays (6, N) (device tensor of the grid's precision).
+
+    ``integrator`` is 'rkn' (fourth-order Runge-Kutta-Nystrom, three field
+    samples per step, the default) or 'rk4' (classical RK4, four samples).
 
     Returns a dict of device tensors: jones [S,4,N], optional state [S,6,N],
     phase [S,N] (float64), amp [S,N], status [N] (uint8), steps [N] (int32),
@@ -239,6 +250,7 @@ def trace(grid: DeviceGrid, rays: torch.Tensor, sched: Schedule, *, axis=2, proj
         p.kappa_q2, p.coulomb_log_w, p.ope_ratio2 = 0.0, 2.0, physics.ope_ratio2(grid.omega)
     p.q_max = float(grid.q_max)
     p.q_min = float(grid.q_min)
+    p.integrator = integrator_code(integrator)
     out = capi.SlothTraceOutputs()
     out.jones = capi.ptr(jones)
     out.state = capi.ptr(state)

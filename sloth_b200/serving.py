@@ -180,6 +180,14 @@ class RayServer:
         capi.check(self.lib.sloth_server_release(self.handle, job.id), "sloth_server_release")
         self.jobs.pop(job.id, None)
 
+    def cancel(self, job: Job):
+        """Cancel a PENDING, RUNNING or DONE job (sloth_server_cancel): it gets
+        no further tiles, and its device memory is released once the
+        iterations already holding its tiles have finished."""
+        capi.check(self.lib.sloth_server_cancel(self.handle, job.id), "sloth_server_cancel")
+        job.keep = []
+        job.state = capi.SLOTH_JOB_CANCELLED
+
     def stats(self) -> dict:
         st = capi.SlothServerStats()
         capi.check(self.lib.sloth_server_stats(self.handle, ctypes.byref(st)), "sloth_server_stats")

@@ -24,7 +24,7 @@ def test_library_exports_every_symbol():
 
 def test_no_device_calls_are_safe():
     lib = _capi.load()
-    assert lib.sloth_abi_version() == 2
+    assert lib.sloth_abi_version() == 3
     assert "sm_100" in _capi.strerror(_capi.SLOTH_ERR_UNSUPPORTED_DEVICE)
     assert _capi.strerror(12345) == "unknown error code"
     # size queries need no device

@@ -159,3 +159,101 @@ def test_job_without_rays_in_the_mix():
     assert e["jones"].shape == (3, 4, 0) and e["phase"].shape == (3, 0) and e["amp"].shape == (3, 0)
     assert e["status"].shape == (0,) and int(e["total_steps"][0]) == 0
     _same(res[job.id], _direct(fields, kind, n, rays))
+
+
+def test_arrivals_while_others_run():
+    """Jobs B and C arrive after job A's first iteration has been launched and
+    while A is still RUNNING; they are admitted into the following
+    iterations beside A's remaining tiles. Every result is bitwise the job's
+    single-trace result."""
+    specs = [("kolmogorov", 48, 40000, 11), ("sinusoid", 64, 6000, 12), ("kolmogorov", 32, 9000, 13)]
+    fields = _fields(specs)
+    with serving.RayServer(2 << 30, tiles_per_step=8, quantum=1) as srv:
+        a, rays_a = _submit(srv, fields, *specs[0])
+        srv.step()                                   # admits A, launches its first iteration
+        assert srv.state(a) == _capi.SLOTH_JOB_RUNNING
+        late = [_submit(srv, fields, *sp) for sp in specs[1:]]
+        overlap = False
+        left = {a.id: a, **{j.id: j for j, _ in late}}
+        while left:
+            srv.step()
+            states = {j.id: srv.state(j) for j in left.values()}
+            if states.get(a.id) == _capi.SLOTH_JOB_RUNNING and any(
+                    states.get(j.id) == _capi.SLOTH_JOB_RUNNING for j, _ in late):
+                overlap = True
+            for jid, st in states.items():
+                if st == _capi.SLOTH_JOB_DONE:
+                    srv.fetch(left[jid])
+                elif st == _capi.SLOTH_JOB_FETCHED:
+                    left.pop(jid)
+        assert overlap, "no late job ran beside A"
+        assert srv.stats()["iterations"] >= 5
+    _same(a.out, _direct(fields, specs[0][0], specs[0][1], rays_a))
+    for (kind, n, _, _), (j, rays) in zip(specs[1:], late):
+        _same(j.out, _direct(fields, kind, n, rays))
+
+
+def test_cancel_pending_running_and_done_jobs():
+    """One table slot: A runs while B waits. A is cancelled mid-run (no
+    further tiles; its memory is released after its in-flight iterations
+    finish), B is cancelled while PENDING and never runs, C is traced after
+    them and matches its single-trace result bitwise, D is cancelled once
+    DONE. At the end the arena holds only the resident grids."""
+    specs = [("kolmogorov", 48, 60000, 21), ("kolmogorov", 48, 5000, 22), ("kolmogorov", 48, 7000, 23),
+             ("kolmogorov", 48, 3000, 24)]
+    fields = _fields(specs)
+    grid_bytes = 48 ** 3 * 16
+    with serving.RayServer(1 << 30, max_jobs=1, tiles_per_step=4, quantum=1) as srv:
+        a, _ = _submit(srv, fields, *specs[0])
+        b, _ = _submit(srv, fields, *specs[1])
+        srv.step()
+        assert srv.state(a) == _capi.SLOTH_JOB_RUNNING and srv.state(b) == _capi.SLOTH_JOB_PENDING
+        srv.cancel(b)
+        srv.step()
+        srv.cancel(a)
+        assert srv.state(a) == _capi.SLOTH_JOB_CANCELLED and srv.state(b) == _capi.SLOTH_JOB_CANCELLED
+        c, rays_c = _submit(srv, fields, *specs[2])
+        res = srv.run_until_done([c])
+        srv.sync()
+        srv.step()                                    # retires A's last iterations
+        st = srv.stats()
+        assert st["cancelled_pending_free"] == 0 and st["jobs_cancelled"] == 2
+        assert st["arena_used"] == grid_bytes
+        d, _ = _submit(srv, fields, *specs[3])
+        while srv.state(d) != _capi.SLOTH_JOB_DONE:
+            srv.step()
+        assert srv.stats()["arena_used"] > grid_bytes
+        srv.cancel(d)
+        assert srv.state(d) == _capi.SLOTH_JOB_CANCELLED
+        st = srv.stats()
+        assert st["arena_used"] == grid_bytes and st["jobs_cancelled"] == 3
+        assert st["jobs_admitted"] == 3                # B never ran
+        for j in (a, b, d):
+            srv.release(j)
+    _same(res[c.id], _direct(fields, specs[2][0], specs[2][1], rays_c))
+
+
+def test_injected_allocation_failure_at_create():
+    """Each of sloth_server_create's allocations, made to fail in turn, ends
+    the create with SLOTH_ERR_OUT_OF_MEMORY and releases everything it had
+    allocated; a server created afterwards works."""
+    lib = _capi.load()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    n_allocs = lib.sloth_server_inject_alloc_failure(0)
+    assert n_allocs >= 5
+    for k in range(1, n_allocs + 1):
+        lib.sloth_server_inject_alloc_failure(k)
+        with pytest.raises(_capi.SlothError) as e:
+            serving.RayServer(256 << 20, tiles_per_step=16)
+        assert e.value.code == _capi.SLOTH_ERR_OUT_OF_MEMORY, k
+    lib.sloth_server_inject_alloc_failure(0)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert abs(free0 - free1) < (64 << 20)            # the 256 MB arena was released every time
+    specs = [("sinusoid", 40, 2000, 31)]
+    fields = _fields(specs)
+    with serving.RayServer(256 << 20, tiles_per_step=16) as srv:
+        job, rays = _submit(srv, fields, *specs[0])
+        res = srv.run_until_done([job])
+    _same(res[job.id], _direct(fields, specs[0][0], specs[0][1], rays))
