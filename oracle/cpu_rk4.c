@@ -41,6 +41,8 @@ typedef struct {
     int32_t inv_brems, early_exit;
     int32_t threads;        /* <= 0: all online cores */
     double plane;
+    int32_t integrator;     /* 0: Runge-Kutta-Nystrom (3 samples), 1: classical RK4 (4 samples) */
+    int32_t pad2;
 } OracleParams;
 
 typedef struct {
@@ -167,6 +169,38 @@ static void step_rkn(const OracleParams* p, double h, int clip, double r[3], dou
     *ta += h / 6.0 * (k1 + 4.0 * k2 + k3);
 }
 
+/* One classical RK4 step of length h of the first-order system (r, v)' =
+ * (v, grad G(r)) with the phase and the depth on RK4's weights:
+ *   r2 = r + h/2 v, v2 = v + h/2 a1;  r3 = r + h/2 v2, v3 = v + h/2 a2;
+ *   r4 = r + h v3, v4 = v + h a3;  r' = r + h/6 (v + 2 v2 + 2 v3 + v4),
+ *   v' = v + h/6 (a1 + 2 a2 + 2 a3 + a4). */
+static void step_rk4(const OracleParams* p, double h, int clip, double r[3], double v[3], double* ph, double* ta) {
+    double a1[3], a2[3], a3[3], a4[3], r2[3], v2[3], r3[3], v3[3], r4[3], v4[3];
+    double g1, g2, g3, g4, k1, k2, k3, k4;
+    rhs(p, r, clip, a1, &g1, &k1);
+    for (int a = 0; a < 3; ++a) {
+        r2[a] = r[a] + 0.5 * h * v[a];
+        v2[a] = v[a] + 0.5 * h * a1[a];
+    }
+    rhs(p, r2, clip, a2, &g2, &k2);
+    for (int a = 0; a < 3; ++a) {
+        r3[a] = r[a] + 0.5 * h * v2[a];
+        v3[a] = v[a] + 0.5 * h * a2[a];
+    }
+    rhs(p, r3, clip, a3, &g3, &k3);
+    for (int a = 0; a < 3; ++a) {
+        r4[a] = r[a] + h * v3[a];
+        v4[a] = v[a] + h * a3[a];
+    }
+    rhs(p, r4, clip, a4, &g4, &k4);
+    for (int a = 0; a < 3; ++a) {
+        r[a] += h / 6.0 * (v[a] + 2.0 * v2[a] + 2.0 * v3[a] + v4[a]);
+        v[a] += h / 6.0 * (a1[a] + 2.0 * a2[a] + 2.0 * a3[a] + a4[a]);
+    }
+    *ph += h / 6.0 * (g1 + 2.0 * g2 + 2.0 * g3 + g4);
+    *ta += h / 6.0 * (k1 + 2.0 * k2 + 2.0 * k3 + k4);
+}
+
 /* A ray inside the grid whose straight-line prediction leaves it within the
  * step takes a step shortened to the face (the RHS is discontinuous there)
  * and is then frozen at time step + phi; a ray outside on an axis and moving
@@ -228,7 +262,10 @@ static long long trace_one(const OracleParams* p, const double* rays, int64_t n,
             }
             const int split = phi < 1.0;
             if (phi < 0.0) phi = 0.0;
-            step_rkn(p, dt * phi, split || near, r, v, &ph, &ta);
+            if (p->integrator == 1)
+                step_rk4(p, dt * phi, split || near, r, v, &ph, &ta);
+            else
+                step_rkn(p, dt * phi, split || near, r, v, &ph, &ta);
             ++nst;
             if (split) frozen_t = (double)step + phi;
         }

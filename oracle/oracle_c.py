@@ -23,7 +23,7 @@ class OracleParams(Structure):
                 ("fields", c_void_p), ("kappa", c_void_p), ("omega", c_double), ("dt", c_double),
                 ("first_save", c_int32), ("save_every", c_int32), ("n_saves", c_int32),
                 ("axis", c_int32), ("project", c_int32), ("inv_brems", c_int32), ("early_exit", c_int32),
-                ("threads", c_int32), ("plane", c_double)]
+                ("threads", c_int32), ("plane", c_double), ("integrator", c_int32), ("pad2", c_int32)]
 
 
 _lib = None
@@ -53,8 +53,9 @@ def threads() -> int:
 
 
 def trace_rays(grid: "rr.Grid", rays, *, dtau, first_save, save_every, n_saves, axis=2, project=False,
-               plane=0.0, inv_brems=False, early_exit=True, threads=0, want_state=True):
-    """C version of ref_restated.trace_rays (phase_mode 'kernel')."""
+               plane=0.0, inv_brems=False, early_exit=True, threads=0, want_state=True, integrator="rkn"):
+    """C version of ref_restated.trace_rays (phase_mode 'kernel'); integrator
+    'rkn' (Runge-Kutta-Nystrom, 3 samples) or 'rk4' (classical RK4, 4)."""
     lib = load()
     rays = np.ascontiguousarray(rays, dtype=np.float64)
     n = rays.shape[1]
@@ -75,6 +76,7 @@ def trace_rays(grid: "rr.Grid", rays, *, dtau, first_save, save_every, n_saves, 
     p.axis, p.project, p.inv_brems, p.early_exit = axis, int(project), int(inv_brems), int(early_exit)
     p.threads = threads
     p.plane = plane
+    p.integrator = {"rkn": 0, "rk4": 1}[integrator]
     S = n_saves
     state = np.zeros((S, 6, n)) if want_state else None
     jones = np.zeros((S, 4, n))

@@ -276,7 +276,7 @@ def phase_integrand(ne_interp, omega, nc):
 
 def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=2,
                project=False, plane=0.0, inv_brems=False, early_exit=True,
-               phase_mode="kernel"):
+               phase_mode="kernel", integrator="rkn"):
     """Fixed-step fourth-order Runge-Kutta-Nystrom integration of dsdt
     (+ phase, + optical depth) in SI units: three samples per step,
     r2 = r + h/2 v + h^2/8 a1, r3 = r + h v + h^2/2 a2, r' = r + h v +
@@ -297,6 +297,8 @@ def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=
     from inside, as an event-locating adaptive solver does. kappa is the reference's interpolated kappa
     grid; phase_mode 'kernel' takes n from the interpolated density,
     'reference' interpolates the (n - 1) grid (full_solver.py:289).
+    integrator 'rk4' takes classical RK4 steps of the first-order system
+    instead (four samples, RK4's weights (1, 2, 2, 1)/6 for the integrals).
     Returns a dict of arrays.
     """
     rays = np.asarray(rays, dtype=np.float64)
@@ -386,14 +388,26 @@ def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=
             # Nystrom's fourth-order Runge-Kutta-Nystrom step (r'' = a(r);
             # three samples), Simpson's weights for the phase and the depth
             a1, g1, k1 = rhs(rr, clamp)
-            r2 = rr + 0.5 * h * vv + (h * h / 8.0) * a1
-            a2, g2, k2 = rhs(r2, clamp)
-            r3 = rr + h * vv + (h * h / 2.0) * a2
-            a3, g3, k3 = rhs(r3, clamp)
-            r[:, idx] = rr + h * vv + (h * h / 6.0) * (a1 + 2 * a2)
-            v[:, idx] = vv + h / 6.0 * (a1 + 4 * a2 + a3)
-            phase[idx] += h / 6.0 * (g1 + 4 * g2 + g3)
-            tau[idx] += h / 6.0 * (k1 + 4 * k2 + k3)
+            if integrator == "rk4":
+                r2, v2 = rr + 0.5 * h * vv, vv + 0.5 * h * a1
+                a2, g2, k2 = rhs(r2, clamp)
+                r3, v3 = rr + 0.5 * h * v2, vv + 0.5 * h * a2
+                a3, g3, k3 = rhs(r3, clamp)
+                r4, v4 = rr + h * v3, vv + h * a3
+                a4, g4, k4 = rhs(r4, clamp)
+                r[:, idx] = rr + h / 6.0 * (vv + 2 * v2 + 2 * v3 + v4)
+                v[:, idx] = vv + h / 6.0 * (a1 + 2 * a2 + 2 * a3 + a4)
+                phase[idx] += h / 6.0 * (g1 + 2 * g2 + 2 * g3 + g4)
+                tau[idx] += h / 6.0 * (k1 + 2 * k2 + 2 * k3 + k4)
+            else:
+                r2 = rr + 0.5 * h * vv + (h * h / 8.0) * a1
+                a2, g2, k2 = rhs(r2, clamp)
+                r3 = rr + h * vv + (h * h / 2.0) * a2
+                a3, g3, k3 = rhs(r3, clamp)
+                r[:, idx] = rr + h * vv + (h * h / 6.0) * (a1 + 2 * a2)
+                v[:, idx] = vv + h / 6.0 * (a1 + 4 * a2 + a3)
+                phase[idx] += h / 6.0 * (g1 + 4 * g2 + g3)
+                tau[idx] += h / 6.0 * (k1 + 4 * k2 + k3)
             steps[idx] += 1
             if split.any():
                 sidx = idx[split]

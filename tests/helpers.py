@@ -47,12 +47,12 @@ def oracle_grid(ne, origin, spacing, omega, Te=None, Z=None):
 
 
 def run_kernel(ne, rays, origin, spacing, omega, sched, *, precision, axis=2, project=False, plane=0.0,
-               inv_brems=False, Te=None, Z=None, want_state=True):
+               inv_brems=False, Te=None, Z=None, want_state=True, integrator="rkn"):
     g = runtime.pack_grid(torch.from_numpy(ne), origin, spacing, omega, precision=precision)
     dt = torch.float32 if precision == "f32" else torch.float64
     r = torch.from_numpy(rays).to("cuda", dt)
     out = runtime.trace(g, r, sched, axis=axis, project=project, plane=plane, inv_brems=inv_brems, Te=Te, Z=Z,
-                        want_state=want_state)
+                        want_state=want_state, integrator=integrator)
     torch.cuda.synchronize()
     res = {k: v.cpu().numpy() for k, v in out.items()}
     res["total_steps"] = int(res["total_steps"][0])
@@ -60,11 +60,11 @@ def run_kernel(ne, rays, origin, spacing, omega, sched, *, precision, axis=2, pr
 
 
 def run_oracle(ne, rays, origin, spacing, omega, sched, *, axis=2, project=False, plane=0.0, inv_brems=False,
-               Te=None, Z=None):
+               Te=None, Z=None, integrator="rkn"):
     grid = oracle_grid(ne, origin, spacing, omega, Te=Te, Z=Z)
     return oracle_c.trace_rays(grid, rays.astype(np.float64), dtau=sched.dtau, first_save=sched.first_save,
                                save_every=sched.save_every, n_saves=sched.n_saves, axis=axis, project=project,
-                               plane=plane, inv_brems=inv_brems)
+                               plane=plane, inv_brems=inv_brems, integrator=integrator)
 
 
 def position_error(got_state, ref_state, L):

@@ -51,8 +51,9 @@ def test_config_sinusoid_slab_128_1e4_rays(precision):
     assert (k["steps"] != o["steps"]).mean() < 1e-3
 
 
+@pytest.mark.parametrize("integ", ["rkn", "rk4"])
 @pytest.mark.parametrize("precision", ["f64", "f32"])
-def test_config_trough_256_lattice(precision):
+def test_config_trough_256_lattice(precision, integ):
     n, n0, Lp = 256, 5e24, 2e-3
     h = L / (n - 1)
     # the quadratic in FP64: differences of float32-rounded densities would
@@ -64,8 +65,8 @@ def test_config_trough_256_lattice(precision):
     rays = rays64.astype(np.float32)
     tau_mid = 0.5 * L
     sched = runtime.schedule_times(np.array([tau_mid]), (h, h, h))
-    k = run_kernel(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched, precision=precision)
-    o = run_oracle(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched)
+    k = run_kernel(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched, precision=precision, integrator=integ)
+    o = run_oracle(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched, integrator=integ)
     assert position_error(k["state"], o["state"], L) < _tol(precision)
     assert direction_error(k["state"], o["state"]) < _tol(precision)
     # analytic x(t) for rays that stay out of the outer cells, at the
@@ -82,17 +83,20 @@ def test_config_trough_256_lattice(precision):
     assert dx < (1e-9 if precision == "f64" else 1e-6), dx
 
 
+@pytest.mark.parametrize("integ", ["rkn", "rk4"])
 @pytest.mark.parametrize("precision", ["f64", "f32"])
-def test_kolmogorov_128_with_absorption(precision):
+def test_kolmogorov_128_with_absorption(precision, integ):
     """The headline mode at a size where interior runs are long: a 128^3
     Kolmogorov box (20% RMS), inverse bremsstrahlung at Te = 20 eV, Z = 1,
-    2e4 rays of a 3 mm beam, three saves; against the oracle."""
+    2e4 rays of a 3 mm beam, three saves; against the oracle, with either
+    integrator (Runge-Kutta-Nystrom, or the classical RK4 the workload
+    descriptions name)."""
     n = 128
     h = L / (n - 1)
     ne = workloads.kolmogorov_box(n, L=L, mean=1e25, rms=0.2, seed=31).numpy()
     rays = workloads.gaussian_beam(20_000, waist=1.5e-3, L=L, seed=32).numpy()
     sched = runtime.schedule_times(np.linspace(0.0, L, 3), (h, h, h))
-    kw = dict(project=True, plane=L / 2, inv_brems=True, Te=20.0, Z=1.0)
+    kw = dict(project=True, plane=L / 2, inv_brems=True, Te=20.0, Z=1.0, integrator=integ)
     k = run_kernel(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched, precision=precision, **kw)
     o = run_oracle(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched, **kw)
     assert position_error(k["state"], o["state"], L) < _tol(precision)

@@ -105,11 +105,12 @@ def _assert_jones(got, ref, pos_atol, ang_atol):
     np.testing.assert_allclose(got[..., [1, 3], :], ref[..., [1, 3], :], rtol=0, atol=ang_atol)
 
 
-def test_trough_matches_reference_and_analytic():
+@pytest.mark.parametrize("integ", ["rkn", "rk4"])
+def test_trough_matches_reference_and_analytic(integ):
     t = golden("trace_cases")
     grid = _trough_grid(float(t["trough_ne0"]), 24, 24)
     sch = _depth_schedule(grid, t["trough_depths"])
-    res = rr.trace_rays(grid, t["trough_s0"].astype(np.float64), **sch)
+    res = rr.trace_rays(grid, t["trough_s0"].astype(np.float64), integrator=integ, **sch)
     x0 = np.array([0.5e-3, 1.0e-3, 1.5e-3, 2.0e-3])
     # reference (DOP853) vs the fixed-step integrator, and analytic SHM x0*cos(pi/4)
     _assert_jones(res["jones"][-1], t["trough_jvec"][-1], 2e-9, 2e-8)
@@ -119,18 +120,20 @@ def test_trough_matches_reference_and_analytic():
     np.testing.assert_allclose(res["jones"][-1][1] * C, -x0 * omega_osc * np.sin(np.pi / 4), rtol=0.10)
 
 
-def test_trough_inv_brems_matches_reference():
+@pytest.mark.parametrize("integ", ["rkn", "rk4"])
+def test_trough_inv_brems_matches_reference(integ):
     t = golden("trace_cases")
     grid = _trough_grid(float(t["trough_ne0"]), 20, 20, Te=100.0, Z=1.0)
     sch = _depth_schedule(grid, t["trough_ib_depths"])
-    res = rr.trace_rays(grid, t["trough_s0"].astype(np.float64), inv_brems=True, **sch)
+    res = rr.trace_rays(grid, t["trough_s0"].astype(np.float64), inv_brems=True, integrator=integ, **sch)
     _assert_jones(res["jones"], t["trough_ib_jvec"], 5e-9, 2e-8)
     # kappa(r) along a path is only piecewise smooth (trilinear, kinks at cell
     # faces): the fixed-step quadrature differs from tight DOP853 by ~1e-5 here.
     np.testing.assert_allclose(res["amp"], t["trough_ib_amp"], rtol=0, atol=2e-5)
 
 
-def test_uniform_absorption_matches_reference_and_formula():
+@pytest.mark.parametrize("integ", ["rkn", "rk4"])
+def test_uniform_absorption_matches_reference_and_formula(integ):
     t = golden("trace_cases")
     n, half = 16, 3e-3
     coords = np.linspace(-half, half, n).astype(np.float32)
@@ -139,7 +142,7 @@ def test_uniform_absorption_matches_reference_and_formula():
     grid = rr.Grid(np.full((n, n, n), 1e25, dtype=np.float32), (float(coords[0]),) * 3, (h,) * 3, omega,
                    Te=100.0, Z=1.0)
     sch = _depth_schedule(grid, t["uniform_depths"])
-    res = rr.trace_rays(grid, t["uniform_s0"].astype(np.float64), inv_brems=True, **sch)
+    res = rr.trace_rays(grid, t["uniform_s0"].astype(np.float64), inv_brems=True, integrator=integ, **sch)
     np.testing.assert_allclose(res["amp"], t["uniform_amp"], rtol=0, atol=5e-9)   # float32 kappa grid in the reference
     _assert_jones(res["jones"], t["uniform_jvec"], 1e-9, 5e-9)
     # amp = exp(-kappa*d/c) of the reference test (5 %): exact here up to n < 1
@@ -147,7 +150,8 @@ def test_uniform_absorption_matches_reference_and_formula():
     assert res["amp"][-1].mean() == pytest.approx(np.exp(-kappa * 2e-3 / C), rel=1e-4)
 
 
-def test_solve_end_state_matches_reference():
+@pytest.mark.parametrize("integ", ["rkn", "rk4"])
+def test_solve_end_state_matches_reference(integ):
     """solve() integrates to c*t = sqrt(8)*depth and reports the current plane."""
     t = golden("trace_cases")
     grid = _trough_grid(float(t["trough_ne0"]), 24, 24)
@@ -155,7 +159,7 @@ def test_solve_end_state_matches_reference():
     h = 0.5 * min(grid.spacing)
     m = int(np.ceil(T / h - 1e-9))
     res = rr.trace_rays(grid, t["trough_s0"].astype(np.float64), dtau=T / m, first_save=m, save_every=1,
-                        n_saves=1)
+                        n_saves=1, integrator=integ)
     _assert_jones(res["jones"][-1], t["solve_rf"], 5e-9, 2e-8)
 
 
@@ -183,12 +187,14 @@ def _sinus_case(n=24, nrays=200, seed=3, axis=2, Te=None):
     return grid, rays
 
 
-@pytest.mark.parametrize("axis,project,ib", [(2, False, False), (0, True, True), (1, False, True)])
-def test_c_oracle_matches_numpy_oracle(axis, project, ib):
+@pytest.mark.parametrize("axis,project,ib,integ", [(2, False, False, "rkn"), (0, True, True, "rkn"),
+                                                   (1, False, True, "rkn"), (2, True, True, "rk4"),
+                                                   (0, False, False, "rk4")])
+def test_c_oracle_matches_numpy_oracle(axis, project, ib, integ):
     grid, rays = _sinus_case(axis=axis, Te=20.0 if ib else None)
     h = 0.5 * min(grid.spacing)
     kw = dict(dtau=h, first_save=0, save_every=60, n_saves=5, axis=axis, project=project, plane=2.5e-3,
-              inv_brems=ib)
+              inv_brems=ib, integrator=integ)
     a = rr.trace_rays(grid, rays, **kw)
     b = oracle_c.trace_rays(grid, rays, **kw)
     np.testing.assert_allclose(b["state"], a["state"], rtol=1e-12, atol=1e-15)
@@ -220,3 +226,59 @@ def test_vacuum_rays_are_straight():
     res = oracle_c.trace_rays(grid, rays, dtau=4e-3 / 60, first_save=60, save_every=1, n_saves=1)
     np.testing.assert_allclose(res["jones"][0][0], rays[0], atol=1e-15)
     assert (res["phase"] == 0).all()
+
+
+PHASE_CASES = ("smooth_532", "dense_1064", "holes_532")
+
+
+@pytest.mark.parametrize("name", PHASE_CASES)
+def test_reference_phase_integrand_golden(name):
+    """The oracle's reference-semantics phase integrand, omega * (interp(n - 1)),
+    equals the legacy solver's own ScalarDomain.phase (src/legacy/full_solver.py:342-345,
+    interp(n) - 1 with fill n = 1) at inside, outside, node and face points."""
+    g = golden("phase")
+    ne, pts, ref = g[f"{name}_ne"], g[f"{name}_points"], g[f"{name}_phase"]
+    ax = [g[f"{name}_{a}"] for a in "xyz"]
+    grid = rr.Grid(ne, [a[0] for a in ax], [a[1] - a[0] for a in ax], float(g[f"{name}_omega"]))
+    _, _, nm1 = grid.sample(pts, with_nm1=True)
+    got = grid.omega * nm1
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() <= 1e-12 * scale
+    outside = np.zeros(pts.shape[1], dtype=bool)
+    for a in range(3):
+        outside |= (pts[a] < ax[a][0]) | (pts[a] > ax[a][-1])
+    assert outside.sum() > 10 and np.all(ref[outside] == 0.0)
+
+
+@pytest.mark.parametrize("name", PHASE_CASES)
+def test_kernel_phase_integrand_equals_reference_at_nodes(name):
+    """The tracers take n from the interpolated density, n(interp(ne)); the
+    legacy solver interpolates n. The two agree at grid nodes, and between
+    nodes differ by the curvature of n(ne) over one cell."""
+    g = golden("phase")
+    ne, pts, ref = g[f"{name}_ne"], g[f"{name}_points"], g[f"{name}_phase"]
+    ax = [g[f"{name}_{a}"] for a in "xyz"]
+    omega = float(g[f"{name}_omega"])
+    grid = rr.Grid(ne, [a[0] for a in ax], [a[1] - a[0] for a in ax], omega)
+    f, _, _ = grid.sample(pts)
+    kern = rr.phase_integrand(f[:, 0], omega, grid.nc)
+    nodes = slice(400, 412)
+    np.testing.assert_allclose(kern[nodes], ref[nodes], rtol=1e-12)
+    gap = np.abs(kern - ref).max() / np.abs(ref).max()
+    assert gap < (0.2 if name == "dense_1064" else 2e-2)
+
+
+def test_rk4_and_rkn_agree():
+    """Both integrators are fourth order in position and direction; on the
+    sinusoid case (h/2 steps) they agree to rounding, and each matches the
+    reference's DOP853 trajectories (the tests above)."""
+    grid, rays = _sinus_case(nrays=60, Te=20.0)
+    L = 5e-3
+    h = 0.5 * min(grid.spacing)
+    m = int(np.ceil(L / h))
+    kw = dict(dtau=L / m, first_save=m, save_every=1, n_saves=1, inv_brems=True)
+    a = oracle_c.trace_rays(grid, rays, integrator="rkn", **kw)
+    b = oracle_c.trace_rays(grid, rays, integrator="rk4", **kw)
+    assert np.array_equal(a["status"], b["status"])
+    assert np.abs(a["state"][-1][:3] - b["state"][-1][:3]).max() / L < 1e-12
+    assert np.abs(a["tau"] - b["tau"]).max() < 1e-9
