@@ -17,7 +17,7 @@ installed either; only their names are needed (`Matrix` is used by the
 reference's unused `ray` helper), so they are empty stand-ins.
 
 Usage (in a container that has the reference at /root/reference):
-    python tests/golden/make_golden.py [/path/to/reference] [--only=diagnostics]
+    python tests/golden/make_golden.py [/path/to/reference] [--only=diagnostics|--only=phase]
 Writes tests/golden/*.npz. The fixtures are committed; nothing on a GPU box
 or in the tests reads the reference tree.
 """
@@ -191,6 +191,9 @@ def main():
     if ONLY == "diagnostics":
         diagnostics_golden()
         return
+    if ONLY == "phase":
+        phase_golden()
+        return
     import core.interpolator as ci           # noqa: E402
     import core.propagator as cp             # noqa: E402
     import shared.propagation as sp          # noqa: E402
@@ -269,7 +272,63 @@ def main():
     tr = _trace_cases(cp, c)
     np.savez(os.path.join(OUT, "trace_cases.npz"), **tr)
     diagnostics_golden()
+    phase_golden()
     print("golden vectors written to", OUT)
+
+
+def phase_golden():
+    """The phase integrand of the legacy full solver, ScalarDomain.phase
+    (src/legacy/full_solver.py:342-345): omega * (interp(n)(x) - 1), with n
+    the refractive index on the grid points (:292-296, NRL omega_pe :236-239)
+    and the interpolator's fill value 1.0 outside the grid (:289).
+
+    The module imports only numpy and scipy, so it runs as shipped except for
+    one defect: omega_pe is declared without `self` (:236) while n_refrac and
+    kappa call it as a method, which raises TypeError. Binding it as a
+    staticmethod fixes that call and changes nothing else.
+
+    The grids have a power-of-two spacing with half-integer or integer
+    offsets, so the float32 coordinates the legacy domain keeps (:118) are
+    exactly the uniform float64 ones."""
+    sys.path.insert(0, os.path.join(REF, "src", "legacy"))
+    import full_solver as fs                 # noqa: E402
+    from scipy.constants import c            # noqa: E402
+    fs.ScalarDomain.omega_pe = staticmethod(fs.ScalarDomain.omega_pe)
+    rng = np.random.RandomState(2718)
+    h = 2.0 ** -13                           # 122 um
+    out = {}
+    for name, shape, lwl, dens in (("smooth_532", (9, 10, 11), 532e-9, "smooth"),
+                                   ("dense_1064", (8, 7, 9), 1064e-9, "dense"),
+                                   ("holes_532", (10, 8, 8), 532e-9, "holes")):
+        coords = [(np.arange(m) - (m - 1) / 2.0) * h for m in shape]
+        omega = 2 * np.pi * c / lwl
+        nc = 3.14207787e-4 * omega ** 2
+        if dens == "smooth":
+            ne = rng.uniform(1e24, 5e25, size=shape)
+        elif dens == "dense":
+            ne = rng.uniform(0.1, 0.9, size=shape) * nc
+        else:
+            ne = rng.uniform(1e24, 5e25, size=shape) * (rng.uniform(size=shape) > 0.3)
+        dom = fs.ScalarDomain(*coords, float(coords[0][-1]), phaseshift=True)
+        dom.external_ne(ne)
+        dom.calc_dndr(lwl)
+        lo = np.array([a[0] for a in coords])
+        hi = np.array([a[-1] for a in coords])
+        inside = lo[:, None] + (hi - lo)[:, None] * rng.uniform(size=(3, 300))
+        around = lo[:, None] - 0.1 * (hi - lo)[:, None] + 1.2 * (hi - lo)[:, None] * rng.uniform(size=(3, 100))
+        idx = [rng.randint(0, m, 12) for m in shape]
+        nodes = np.stack([coords[a][idx[a]] for a in range(3)])
+        faces = inside[:, :12].copy()
+        for k in range(12):
+            faces[k % 3, k] = (lo if k % 2 else hi)[k % 3]
+        pts = np.concatenate([inside, around, nodes, faces], axis=1)
+        out[f"{name}_ne"] = ne
+        out[f"{name}_x"], out[f"{name}_y"], out[f"{name}_z"] = coords
+        out[f"{name}_omega"] = np.float64(dom.omega)
+        out[f"{name}_points"] = pts
+        out[f"{name}_phase"] = np.asarray(dom.phase(pts), dtype=np.float64)
+    np.savez(os.path.join(OUT, "phase.npz"), **out)
+    print("phase golden vectors written to", OUT)
 
 
 def _trough_domain(c, ne_0, a, half_z, n_xy, n_z, inv_brems=False, Te=None, Z=None):
