@@ -8,7 +8,8 @@ Mirrors the reference's public functions (src/core/propagator.py):
 * ``solve``                                           (:364-929)
 * ``trace_and_save_depths``                           (:932-1234)
 
-with the same signatures, return values and errors. The ODE is integrated
+with the same signatures, return values and errors (plus keyword-only
+extras, below). The ODE is integrated
 with a fixed-step fourth-order Runge-Kutta-Nystrom method (step = half the
 smallest grid spacing, in c*t) by the sm_100a tracers instead of diffrax's
 adaptive Tsit5, so ``jitted``, ``parallelise``, ``rtol`` and ``atol`` are
@@ -16,7 +17,12 @@ accepted and have no effect.
 Additive keyword-only extras: ``precision`` ('f32' = FP32 kernel with
 compensated sums and FP64 phase, 'f64' = all-FP64 kernel), ``detector_plane``
 (back-project the final rays to that plane), ``return_extras`` (append a dict
-with the optical phase, per-ray status and step counts), ``device``, ``stream``.
+with the optical phase, per-ray status and step counts), ``integrator``
+('rkn', the default, or 'rk4': classical RK4 steps, four field samples
+instead of three), ``device``, ``stream``,
+``group`` (a torch.distributed process group: the job's rays are split over
+its ranks, each rank traces its slice through its own copy of the grid, and
+every rank returns the results of all rays in their order; see shard.py).
 """
 from __future__ import annotations
 
@@ -27,7 +33,7 @@ import warnings
 import numpy as np
 import torch
 
-from .. import runtime
+from .. import runtime, shard
 from ..shared.propagation import ray_to_Jonesvector, back_propogate  # noqa: F401  (re-exported as in the reference)
 from . import physics
 from .beam import Beam
@@ -173,10 +179,27 @@ class RawSolution:
 # ---------------------------------------------------------------------------
 # solve (propagator.py:364-929)
 # ---------------------------------------------------------------------------
+def _traced(grid, rays, sched, *, want, chunk_rays, group, dev, **kw):
+    """runtime.trace_to_host over all rays, or, with a process group, over this
+    rank's slice followed by the all-gather of every output into ray order
+    (total ray-steps summed, time the longest over the ranks)."""
+    if group is None:
+        return runtime.trace_to_host(grid, rays, sched, want=want, chunk_rays=chunk_rays, **kw)
+    world, rank = shard.group_info(group)
+    n = int(rays.shape[1])
+    lo, hi = shard.shard_bounds(n, world, rank)
+    host, total_steps, duration = runtime.trace_to_host(grid, rays[:, lo:hi], sched, want=want,
+                                                        chunk_rays=chunk_rays, **kw)
+    cdev = shard.comm_device(group, dev)
+    host = {k: shard.gather_rays(v, n, group, cdev) for k, v in host.items()}
+    return host, int(shard.reduce_scalar(total_steps, group, cdev, "sum")), \
+        shard.reduce_scalar(duration, group, cdev, "max")
+
+
 def solve(beam, ScalarDomain, probing_depth, *, parallelise=True, jitted=True, save_points_per_region=2,
           memory_debug=False, lwl=1064e-9, keep_domain=False, return_raw_results=False, verbose=True,
           precision="f32", detector_plane=None, return_extras=False, device=None, stream=None,
-          chunk_rays=None):
+          chunk_rays=None, group=None, integrator="rkn"):
     """Trace rays through the domain to c*t = sqrt(8)*probing_depth (the
     reference's integration end, :616-617) and return (rf, amp, duration).
 
@@ -189,7 +212,9 @@ def solve(beam, ScalarDomain, probing_depth, *, parallelise=True, jitted=True, s
     and results' copies, which overlap it.
 
     The rays pass through the device in chunks of ``chunk_rays`` (default
-    ``runtime.STREAM_CHUNK_RAYS``); the results do not depend on it.
+    ``runtime.STREAM_CHUNK_RAYS``); the results do not depend on it. With a
+    process group every rank passes the same beam and domain; each traces
+    its slice of the rays and returns the results of all of them.
     """
     omega = physics.omega_of(lwl)
     region_count = getattr(ScalarDomain, "region_count", 1)
@@ -219,9 +244,10 @@ def solve(beam, ScalarDomain, probing_depth, *, parallelise=True, jitted=True, s
             want["amp"] = "last"
     if return_extras:
         want.update(phase="all", status="all", steps="all")
-    host, total_steps, duration = runtime.trace_to_host(
-        grid, rays, sched, want=want, chunk_rays=chunk_rays, axis=axis, project=project,
-        plane=float(detector_plane) if project else 0.0, inv_brems=inv_brems, Te=Te, Z=Z, stream=stream)
+    host, total_steps, duration = _traced(
+        grid, rays, sched, want=want, chunk_rays=chunk_rays, group=group, dev=dev, axis=axis, project=project,
+        plane=float(detector_plane) if project else 0.0, inv_brems=inv_brems, Te=Te, Z=Z, stream=stream,
+        integrator=integrator)
     duration = np.float64(duration)
     if verbose:
         print("\nCompleted ray trace in", np.round(duration, 3), "seconds.")
@@ -250,11 +276,12 @@ def solve(beam, ScalarDomain, probing_depth, *, parallelise=True, jitted=True, s
 # ---------------------------------------------------------------------------
 def trace_and_save_depths(beam, ScalarDomain, step, depth_max, output_path, *, lwl=1064e-9, jones_components=None,
                           jitted=True, rtol=1e-3, atol=1e-5, verbose=True, precision="f32", return_extras=False,
-                          device=None, stream=None, chunk_rays=None):
+                          device=None, stream=None, chunk_rays=None, group=None, integrator="rkn"):
     """Trace rays and save the Jones vector at depths 0, step, ..., depth_max
     (c*t = depth, :1133-1138); returns {'depth_saves', 'jvec',
     'jones_components'[, 'amplitude']} and optionally pickles it. The rays
-    pass through the device in chunks of ``chunk_rays``, as in ``solve``."""
+    pass through the device in chunks of ``chunk_rays``, and split over a
+    process group's ranks with ``group``, as in ``solve``."""
     omega = physics.omega_of(lwl)
     s0 = _rays_from(beam, ScalarDomain)
     if step <= 0 or depth_max <= 0:
@@ -292,8 +319,8 @@ def trace_and_save_depths(beam, ScalarDomain, step, depth_max, output_path, *, l
     sched = runtime.schedule_times(depth_saves, grid.spacing)
     want = {k: "all" for k in ["jones"] + (["amp"] if inv_brems else []) +
             (["phase", "status", "steps"] if return_extras else [])}
-    host, _, _ = runtime.trace_to_host(grid, s0, sched, want=want, chunk_rays=chunk_rays, axis=axis,
-                                       inv_brems=inv_brems, Te=Te, Z=Z, stream=stream)
+    host, _, _ = _traced(grid, s0, sched, want=want, chunk_rays=chunk_rays, group=group, dev=dev, axis=axis,
+                         inv_brems=inv_brems, Te=Te, Z=Z, stream=stream, integrator=integrator)
     jones = host["jones"]
     jvec = [np.asarray(jones[j])[comp, :] for j in range(n_saves)]
     result = {'depth_saves': depth_saves, 'jvec': jvec, 'jones_components': comp}
@@ -304,7 +331,7 @@ def trace_and_save_depths(beam, ScalarDomain, step, depth_max, output_path, *, l
         result['phase'] = [p for p in host["phase"]]
         result['status'] = host["status"]
         result['steps'] = host["steps"]
-    if output_path is not None:
+    if output_path is not None and (group is None or shard.group_info(group)[1] == 0):
         with open(output_path, 'wb') as fh:
             pickle.dump(result, fh)
         if verbose:
