@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--rays", type=float, default=1e7)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-rk4", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -64,6 +65,19 @@ def measured_peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def committed_lane_ops():
+    """FP32 lane-operations per ray-step of the trace kernel, from the committed
+    ncu instruction-mix summary (scalar FFMA/FADD/FMUL plus two lanes per
+    paired FFMA2/FADD2/FMUL2)."""
+    p = os.path.join(ROOT, "profiles", "trace_kernel_kolmogorov512_1e7.md")
+    if not os.path.exists(p):
+        return None, None
+    text = open(p).read()
+    m = re.search(r"fp32_lane_ops_per_ray_step:\s*([0-9.eE+]+)", text)
+    w = re.search(r"fp32_lane_ops_workload:\s*(.+)", text)
+    return (float(m.group(1)) if m else None), (w.group(1).strip() if w else None)
 
 
 def committed_traffic(args):
@@ -145,32 +159,49 @@ def make_workload(n, nrays, seed, device):
 # ---------------------------------------------------------------------------
 # reference arm: the oracle's C restatement of the reference on host cores
 # ---------------------------------------------------------------------------
-def cpu_oracle_rate(ne_host, rays_host, spacing, omega, dtau, n_steps, seconds, threads=0):
-    """Time the FP64 C restatement on a bounded ray sample; returns
-    (ray-steps/s, sample description, threads, total_steps)."""
+def cpu_sample(ne_host, rays_host, spacing, omega, dtau, n_steps, seconds, threads=0):
+    """The bounded CPU sample of the workload: the first m rays of the beam, all
+    their steps, with m sized from a short probe so that one trace of the
+    sample takes about `seconds` on the host cores. Returns (run, m, threads),
+    run() tracing the sample once and returning its ray-step count."""
     from oracle import oracle_c
     from oracle import ref_restated as rr
     grid = rr.Grid(ne_host.astype(np.float64), (-L / 2,) * 3, spacing, omega, Te=TE, Z=ZION)
     thr = threads or oracle_c.threads()
-    probe = min(rays_host.shape[1], 64 * thr)
     kw = dict(dtau=dtau, first_save=n_steps, save_every=1, n_saves=1, project=True, plane=L / 2,
               inv_brems=True, threads=thr, want_state=False)
+    probe = min(rays_host.shape[1], 256 * thr)
     t0 = time.perf_counter()
     r = oracle_c.trace_rays(grid, rays_host[:, :probe], **kw)
     dt = time.perf_counter() - t0
-    rate = r["total_steps"] / dt
-    m = int(min(rays_host.shape[1], max(probe, rate * seconds / max(r["total_steps"] / probe, 1))))
+    per_ray_s = dt / probe
+    m = int(min(rays_host.shape[1], max(probe, seconds / per_ray_s)))
+    sub = np.ascontiguousarray(rays_host[:, :m])
+
+    def run():
+        return oracle_c.trace_rays(grid, sub, **kw)["total_steps"]
+    return run, m, thr
+
+
+def cpu_oracle_rate(ne_host, rays_host, spacing, omega, dtau, n_steps, seconds, threads=0):
+    """Time the oracle's FP64 C restatement on the bounded sample once;
+    returns (ray-steps/s, sample description, threads, total_steps)."""
+    run, m, thr = cpu_sample(ne_host, rays_host, spacing, omega, dtau, n_steps, seconds, threads)
     t0 = time.perf_counter()
-    r = oracle_c.trace_rays(grid, rays_host[:, :m], **kw)
+    steps = run()
     dt = time.perf_counter() - t0
-    return r["total_steps"] / dt, f"first {m} rays of the 1e7-ray beam, all steps", thr, r["total_steps"]
+    return steps / dt, f"first {m} rays of the 1e7-ray beam, all steps", thr, steps
 
 
 def run_reference(args):
+    """The reference arm: the oracle's FP64 C restatement of the reference
+    propagator on every host core, each step one trace of the same bounded
+    sample the sloth arm's cpu_baseline leg times (the first m rays of the
+    beam, all steps), m sized so that the W + K steps take about three
+    minutes (at most 15 s per step)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import torch
     from sloth_b200 import runtime, workloads
     from sloth_b200.core import physics
     n = args.n
@@ -179,35 +210,29 @@ def run_reference(args):
     rays = workloads.gaussian_beam(int(args.rays), waist=1.5e-3, L=L, seed=args.seed + 1).double().numpy()
     omega = physics.omega_of(LWL)
     sched = runtime.schedule_times([math.sqrt(8.0) * L], (h, h, h))
-    from oracle import oracle_c
-    from oracle import ref_restated as rr
-    grid = rr.Grid(ne.astype(np.float64), (-L / 2,) * 3, (h, h, h), omega, Te=TE, Z=ZION)
-    thr = oracle_c.threads()
-    per_step = max(64 * thr, 2000)
-    kw = dict(dtau=sched.dtau, first_save=sched.first_save, save_every=1, n_saves=1, project=True, plane=L / 2,
-              inv_brems=True, threads=thr, want_state=False)
+    per_step_s = min(args.cpu_seconds, 180.0 / max(1, args.steps + args.warmup))
+    run, m, thr = cpu_sample(ne, rays, (h, h, h), omega, sched.dtau, sched.first_save, per_step_s)
     times, steps = [], []
     for i in range(args.warmup + args.steps):
-        lo = (i * per_step) % rays.shape[1]
-        sub = rays[:, lo:lo + per_step]
         t0 = time.perf_counter()
-        r = oracle_c.trace_rays(grid, sub, **kw)
+        st = run()
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             times.append(dt)
-            steps.append(r["total_steps"])
+            steps.append(st)
     value = float(np.sum(steps) / np.sum(times))
+    sample = f"first {m} rays of the {int(args.rays):.0e}-ray beam, all steps, traced once per step"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{n}^3 Kolmogorov turbulent box (mean 1e19 cm^-3, 20% RMS), 1e7-ray 3 mm "
-                               f"Gaussian beam, 532 nm, Te=20 eV, Z=1; each step a {per_step}-ray sample",
+        "config": {"workload": f"{n}^3 Kolmogorov turbulent box (mean 1e19 cm^-3, 20% RMS), {int(args.rays):.0e}-ray "
+                               f"3 mm Gaussian beam, 532 nm, Te=20 eV, Z=1; each step the {m}-ray sample",
+                   "integrator": "fixed-step 4th-order Runge-Kutta-Nystrom, ds = h/2",
+                   "field_samples_per_ray_step": 3,
                    "note": "the reference (JAX/diffrax) cannot be installed on this image; its CPU path is "
-                           "stood in for by the oracle's FP64 C restatement (fixed-step 4th-order "
-                           "Runge-Kutta-Nystrom, the tracers' method)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port",
-                         "sample": f"{per_step} rays per step, {args.steps} steps"},
+                           "stood in for by the oracle's FP64 C restatement (the tracers' method)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -354,6 +379,64 @@ def run_adjoint(args):
 
 
 # ---------------------------------------------------------------------------
+# error of the FP32 split kernel against the all-FP64 port (all rays)
+# ---------------------------------------------------------------------------
+def _q(t, p):
+    import torch
+    t = t.float() if t.numel() < 2 ** 24 else t[:: max(1, t.numel() // 2 ** 23)].float()
+    return float(torch.quantile(t, p))
+
+
+def accuracy(o32, o64, spread=None):
+    """Per-output error of the FP32 kernel against the FP64 port on every ray;
+    far-face rays (those crossing the far face inside the box's transverse
+    extent) and side-exit rays (the others, leaving or missing the box
+    through a side face at grazing incidence) are also reported apart.
+    `spread` is the FP64 port's own change when its input positions move by
+    one FP32 ulp (amp and phase, per ray): the conditioning of each ray."""
+    j32, j64 = o32["jones"][-1].double(), o64["jones"][-1].double()
+    ok = (o32["status"] != 2) & (o64["status"] != 2)
+    far = ok & (j64[0].abs() <= L / 2) & (j64[2].abs() <= L / 2)
+    side = ok & ~far
+    dpos = torch_max(j32[0], j64[0], j32[2], j64[2])[ok] / L
+    dang = torch_max(j32[1], j64[1], j32[3], j64[3])[ok]
+    ph64 = o64["phase"][-1]
+    scale = float(ph64[ok].abs().max())
+    dph = (o32["phase"][-1] - ph64).abs()
+    damp = (o32["amp"][-1].double() - o64["amp"][-1].double()).abs()
+    acc = {"position_rel_L_max": float(dpos.max()), "position_rel_L_p99": _q(dpos, 0.99),
+           "angle_abs_max_rad": float(dang.max()), "angle_abs_p99_rad": _q(dang, 0.99),
+           "phase_abs_max_rad": float(dph[ok].max()), "phase_max_abs_rad": scale,
+           "phase_rel_max": float(dph[ok].max()) / scale,
+           "phase_rel_max_far_face": float(dph[far].max()) / scale,
+           "phase_rel_p99": _q(dph[ok] / scale, 0.99),
+           "amp_abs_max": float(damp[ok].max()), "amp_abs_max_far_face": float(damp[far].max()),
+           "amp_abs_p99": _q(damp[ok], 0.99),
+           "rays_compared": int(ok.sum()), "rays_far_face": int(far.sum()), "rays_side_exit": int(side.sum()),
+           "status_mismatch": int((o32["status"] != o64["status"]).sum())}
+    if side.any():
+        acc["amp_abs_max_side_exit"] = float(damp[side].max())
+        acc["phase_rel_max_side_exit"] = float(dph[side].max()) / scale
+    if spread is not None and side.any():
+        s_amp, s_ph = spread
+        big = side & (damp > 1e-6)
+        acc["fp64_one_ulp_input_spread"] = {
+            "what": "the FP64 port's own change when the rays' x and y move by one FP32 ulp (max over +/-)",
+            "amp_abs_max_side_exit": float(s_amp[side].max()), "amp_abs_max_far_face": float(s_amp[far].max()),
+            "phase_rel_max_side_exit": float(s_ph[side].max()) / scale,
+            "phase_rel_max_far_face": float(s_ph[far].max()) / scale,
+            "side_exit_rays_amp_err_above_1e-6": int(big.sum()),
+            "their_fp64_spread_min": float(s_amp[big].min()) if big.any() else None,
+            "side_exit_rays_spread_above_1e-6": int((side & (s_amp > 1e-6)).sum())}
+    return acc
+
+
+def torch_max(a1, b1, a2, b2):
+    import torch
+    return torch.maximum((a1 - b1).abs(), (a2 - b2).abs())
+
+
+# ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
 def run_sloth(args):
@@ -416,59 +499,67 @@ def run_sloth(args):
     f32_out = {k: v.clone() for k, v in outs.items()}
 
     # ---- all-FP64 port of the same kernel on the same workload -------------
-    fp64 = None
-    acc = None
-    if not args.no_fp64 and world == 1:
-        g64 = runtime.pack_grid(ne, (-L / 2,) * 3, (h, h, h), omega, precision="f64")
-        r64 = rays.double()
-        o64 = {}
-        for _ in range(1):
-            runtime.trace(g64, r64, sched, project=True, plane=L / 2, inv_brems=True, Te=TE, Z=ZION,
-                          want_steps=False, outputs=o64)
+    tkw = dict(project=True, plane=L / 2, inv_brems=True, Te=TE, Z=ZION, want_steps=False)
+
+    def timed(g, r, reps, integ, outputs):
+        """Mean ms per trace and mean trace-kernel ms over `reps` traces (after one untimed)."""
+        runtime.trace(g, r, sched, outputs=outputs, integrator=integ, **tkw)
         torch.cuda.synchronize()
         k2 = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
         k2[0].record()
         k2[1].record()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = 2
         ktimes = []
         e0.record(stream)
         for _ in range(reps):
-            runtime.trace(g64, r64, sched, project=True, plane=L / 2, inv_brems=True, Te=TE, Z=ZION,
-                          want_steps=False, outputs=o64, events=k2)
+            runtime.trace(g, r, sched, outputs=outputs, integrator=integ, events=k2, **tkw)
             e1.record(stream)
             torch.cuda.synchronize()
             ktimes.append(k2[0].elapsed_time(k2[1]))
-        ms64 = e0.elapsed_time(e1) / reps
-        rs64 = int(o64["total_steps"][0])
-        fp64 = {"value": rs64 / (ms64 / 1e3), "ms_per_step": ms64, "kernel_ms": float(np.mean(ktimes)),
-                "ray_steps": rs64}
-        # accuracy of the FP32 split kernel against the FP64 port (all rays)
-        j32, j64 = f32_out["jones"][-1].double(), o64["jones"][-1]
-        ok = (f32_out["status"] != 2) & (o64["status"] != 2)
-        # rays that crossed the far face inside the box's transverse extent;
-        # the others left (or never entered) through a side face at grazing incidence
-        far = ok & (j64[0].abs() <= L / 2) & (j64[2].abs() <= L / 2)
-        dpos = torch.maximum((j32[0] - j64[0]).abs(), (j32[2] - j64[2]).abs())[ok] / L
-        dang = torch.maximum((j32[1] - j64[1]).abs(), (j32[3] - j64[3]).abs())[ok]
-        ph64 = o64["phase"][-1][ok]
-        dph = (f32_out["phase"][-1][ok] - ph64).abs()
-        damp = (f32_out["amp"][-1].double() - o64["amp"][-1])[ok].abs()
+        return e0.elapsed_time(e1) / reps, float(np.mean(ktimes))
 
-        def q(t, p):
-            t = t.float() if t.numel() < 2 ** 24 else t[:: max(1, t.numel() // 2 ** 23)].float()
-            return float(torch.quantile(t, p))
-        farm = far[ok]
-        acc = {"position_rel_L_max": float(dpos.max()), "position_rel_L_p99": q(dpos, 0.99),
-               "angle_abs_max_rad": float(dang.max()), "angle_abs_p99_rad": q(dang, 0.99),
-               "phase_abs_max_rad": float(dph.max()), "phase_max_abs_rad": float(ph64.abs().max()),
-               "phase_rel_max": float(dph.max() / ph64.abs().max()),
-               "phase_rel_max_far_face": float(dph[farm].max() / ph64.abs().max()),
-               "phase_rel_p99": q(dph / ph64.abs().max(), 0.99),
-               "amp_abs_max": float(damp.max()), "amp_abs_max_far_face": float(damp[farm].max()),
-               "amp_abs_p99": q(damp, 0.99),
-               "rays_compared": int(ok.sum()), "rays_far_face": int(farm.sum()),
-               "status_mismatch": int((f32_out["status"] != o64["status"]).sum())}
+    fp64 = None
+    acc = None
+    rk4 = None
+    if not args.no_fp64 and world == 1:
+        g64 = runtime.pack_grid(ne, (-L / 2,) * 3, (h, h, h), omega, precision="f64")
+        r64 = rays.double()
+        o64 = {}
+        ms64, kms64 = timed(g64, r64, 2, "rkn", o64)
+        rs64 = int(o64["total_steps"][0])
+        fp64 = {"value": rs64 / (ms64 / 1e3), "ms_per_step": ms64, "kernel_ms": kms64, "ray_steps": rs64}
+        # the FP64 port's sensitivity to a one-ulp (FP32) move of the input positions
+        s_amp = s_ph = None
+        for d in (1.0, -1.0):
+            rp = rays.clone()
+            rp[0:2] = torch.nextafter(rp[0:2], torch.full_like(rp[0:2], d * math.inf))
+            op = runtime.trace(g64, rp.double(), sched, **tkw)
+            da = (op["amp"][-1] - o64["amp"][-1]).abs()
+            dp = (op["phase"][-1] - o64["phase"][-1]).abs()
+            s_amp = da if s_amp is None else torch.maximum(s_amp, da)
+            s_ph = dp if s_ph is None else torch.maximum(s_ph, dp)
+            del op
+        acc = accuracy(f32_out, o64, (s_amp, s_ph))
+        del s_amp, s_ph
+        if not args.no_rk4:
+            # the classical RK4 step the workload descriptions name: four field
+            # samples per ray-step instead of three, FP32 split and FP64 port
+            o4 = {}
+            ms4, kms4 = timed(grid, rays, 3, "rk4", o4)
+            rs4 = int(o4["total_steps"][0])
+            o4_64 = {}
+            ms4_64, kms4_64 = timed(g64, r64, 1, "rk4", o4_64)
+            rk4 = {"integrator": "classical RK4, ds = h/2", "field_samples_per_ray_step": 4,
+                   "value": rs4 / (ms4 / 1e3), "ms_per_step": ms4, "kernel_ms": kms4, "ray_steps": rs4,
+                   "fp64_port": {"value": int(o4_64["total_steps"][0]) / (ms4_64 / 1e3), "ms_per_step": ms4_64,
+                                 "kernel_ms": kms4_64},
+                   "speedup_of_fp32": ms4_64 / ms4,
+                   "fp32_vs_fp64": accuracy(o4, o4_64)}
+            # the two integrators' FP64 results differ by their truncation error
+            j4, jn = o4_64["jones"][-1], o64["jones"][-1]
+            rk4["rkn_vs_rk4_fp64_position_rel_L_max"] = float(
+                torch_max(j4[0], jn[0], j4[2], jn[2]).max() / L)
+            del o4, o4_64
         del g64, r64, o64
 
     # ---- end to end through the public API (host buffers) -------------------
@@ -528,41 +619,59 @@ def run_sloth(args):
         cpu = {"value": rate, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
 
     if rank == 0:
-        peak, peak_kind = measured_peaks()
+        hbm_peak, peak_kind = measured_peaks()
         kms = float(np.mean(kernel_ms))
-        achieved = ray_steps * BYTES_PER_RAY_STEP / (kms / 1e3) / 1e9
         traffic = committed_traffic(args)
+        lane_ops, lane_ops_where = committed_lane_ops()
+        clocks = clk.summary()
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+        # the FP32 pipe: 128 FP32 lanes per SM per clock (FFMA2 occupies both FMA pipes)
+        pipe_peak = sms * 128 * sm_mhz * 1e6 / 1e12
+        pipe_achieved = ray_steps * lane_ops / (kms / 1e3) / 1e12 if lane_ops else None
+        gather_gbs = ray_steps * BYTES_PER_RAY_STEP / (kms / 1e3) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{n}^3 Kolmogorov turbulent box (mean 1e19 cm^-3, 20% RMS, k^-11/3), "
                                    f"{nrays:.0e} rays, 3 mm Gaussian beam along +z, 532 nm, Te=20 eV, Z=1, "
-                                   "fixed-step 4th-order Runge-Kutta-Nystrom ds=h/2, detector plane z=+2.5 mm",
+                                   "detector plane z=+2.5 mm",
+                       "integrator": "fixed-step 4th-order Runge-Kutta-Nystrom, ds = h/2",
+                       "field_samples_per_ray_step": 3,
+                       "unit_of_work": "one ray-step = one fixed step of one ray inside or near the grid; it "
+                                       "samples the field 3 times (RK4 would sample it 4 times)",
                        "l2": f"inputs larger than L2 ({n ** 3 * 16 / 1e9:.2f} GB packed grid, "
                              f"{nrays * 24 / 1e6:.0f} MB rays)",
                        "precision": "FP32 state with compensated sums, FP64 phase, Kahan FP32 optical depth",
                        "seed": args.seed, "ray_steps_per_trace": ray_steps},
             "latency_ms": {"p50": float(np.percentile(per_step_ms, 50)), "p99": float(np.percentile(per_step_ms, 99)),
                            "what": "one 1e7-ray trace per request"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_kind": f"{peak_kind} HBM copy bandwidth",
+            "roofline": {"bound": "fp32_pipe", "achieved": pipe_achieved, "peak": pipe_peak,
+                         "unit": "T FP32 lane-ops/s",
+                         "frac": (pipe_achieved / pipe_peak) if pipe_achieved else None,
+                         "traffic": traffic,
+                         "peak_kind": f"{sms} SMs x 128 FP32 lanes x {sm_mhz:.0f} MHz (median SM clock sampled "
+                                      "in the timed region)",
+                         "lane_ops_per_ray_step": lane_ops, "lane_ops_from": lane_ops_where,
                          "kernel": "trace_kernel<PolF32>", "kernel_ms": kms,
-                         "bytes_per_ray_step": BYTES_PER_RAY_STEP,
-                         "dram_achieved": (traffic / (kms / 1e3) / 1e9) if traffic else None,
-                         "dram_frac": (traffic / (kms / 1e3) / 1e9 / peak) if traffic else None,
-                         "note": "achieved = logical gather bytes (3 stages x 8 corners x 16 B per ray-step); "
-                                 "the corners come from a register cell cache and L1, so physical DRAM traffic "
-                                 "(traffic, dram_frac, from ncu) is ~1.5 B per ray-step; the kernel is bound by "
-                                 "its FP32 pipes: instruction issue at ~59% of peak, FMA pipe ~66% active "
-                                 "(ncu summary in profiles/)"},
+                         "hbm": {"peak_gbs": hbm_peak, "peak_kind": f"{peak_kind} HBM copy bandwidth",
+                                 "dram_achieved_gbs": (traffic / (kms / 1e3) / 1e9) if traffic else None,
+                                 "dram_frac": (traffic / (kms / 1e3) / 1e9 / hbm_peak) if traffic else None,
+                                 "logical_gather_bytes_per_ray_step": BYTES_PER_RAY_STEP,
+                                 "logical_gather_gbs": gather_gbs},
+                         "note": "achieved = ray-steps/s x FP32 lane-operations per ray-step (ncu instruction "
+                                 "mix: scalar FFMA/FADD/FMUL + 2 x paired FFMA2/FADD2/FMUL2); the trace is bound "
+                                 "by its FP32 pipes, not memory: DRAM traffic (traffic, from ncu) is ~1.5 B per "
+                                 "ray-step against 384 logical gather bytes, which a register cell cache and L1 "
+                                 "serve"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),
-            "clocks": clk.summary(),
+            "clocks": clocks,
             "fp64_port": fp64,
             "fp32_vs_fp64": acc,
+            "rk4": rk4,
             "serving": serve,
             "adjoint": adj,
             "diagnostics": diag,

@@ -42,3 +42,16 @@ def test_committed_traffic_only_for_the_profiled_workload():
 def test_logical_bytes_per_ray_step():
     """Three stage samples of eight 16-byte voxels."""
     assert _bench().BYTES_PER_RAY_STEP == 3 * 8 * 16
+
+
+def test_committed_lane_ops_match_the_instruction_mix():
+    """The FP32 lane-operations per ray-step that the roofline uses equal the
+    summary's scalar FP32 count plus two lanes per paired instruction."""
+    ops, where = _bench().committed_lane_ops()
+    text = open(os.path.join(ROOT, "profiles", "trace_kernel_kolmogorov512_1e7.md")).read()
+    m = re.search(r"\| FFMA2 / FADD2 / FMUL2 \(two FP32 lanes each\) \| ([0-9.]+) / ([0-9.]+) / ([0-9.]+)", text)
+    s = re.search(r"\| FFMA / FADD / FMUL \| ([0-9.]+) / ([0-9.]+) / ([0-9.]+)", text)
+    paired = sum(float(x) for x in m.groups())
+    scalar = sum(float(x) for x in s.groups())
+    assert abs(ops - (scalar + 2 * paired)) < 0.5
+    assert where
