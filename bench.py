@@ -180,6 +180,7 @@ def cpu_sample(ne_host, rays_host, spacing, omega, dtau, n_steps, seconds, threa
 
     def run():
         return oracle_c.trace_rays(grid, sub, **kw)["total_steps"]
+    run.grid = grid
     return run, m, thr
 
 
@@ -190,7 +191,7 @@ def cpu_oracle_rate(ne_host, rays_host, spacing, omega, dtau, n_steps, seconds, 
     t0 = time.perf_counter()
     steps = run()
     dt = time.perf_counter() - t0
-    return steps / dt, f"first {m} rays of the 1e7-ray beam, all steps", thr, steps
+    return steps / dt, f"first {m} rays of the 1e7-ray beam, all steps", thr, steps, run.grid
 
 
 def run_reference(args):
@@ -521,6 +522,8 @@ def run_sloth(args):
     fp64 = None
     acc = None
     rk4 = None
+    phase_first = None
+    phase_ref = None
     if not args.no_fp64 and world == 1:
         g64 = runtime.pack_grid(ne, (-L / 2,) * 3, (h, h, h), omega, precision="f64")
         r64 = rays.double()
@@ -541,6 +544,8 @@ def run_sloth(args):
             del op
         acc = accuracy(f32_out, o64, (s_amp, s_ph))
         del s_amp, s_ph
+        phase_first = {"rays": 100, "f64": o64["phase"][-1][:100].cpu().numpy(),
+                       "f32": f32_out["phase"][-1][:100].cpu().numpy()}
         if not args.no_rk4:
             # the classical RK4 step the workload descriptions name: four field
             # samples per ray-step instead of three, FP32 split and FP64 port
@@ -614,9 +619,28 @@ def run_sloth(args):
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, sample, thr, _ = cpu_oracle_rate(ne.cpu().numpy(), rays.double().cpu().numpy(), (h, h, h), omega,
-                                               sched.dtau, sched.first_save, args.cpu_seconds)
+        rays_host = rays.double().cpu().numpy()
+        rate, sample, thr, _, ogrid = cpu_oracle_rate(ne.cpu().numpy(), rays_host, (h, h, h), omega, sched.dtau,
+                                                      sched.first_save, args.cpu_seconds)
         cpu = {"value": rate, "unit": UNIT, "cores": thr, "kind": "port", "sample": sample}
+        if phase_first is not None:
+            # the kernels' phase against the oracle's reference semantics (the
+            # legacy solver's interpolated n, pinned to its own phase()) on
+            # the first rays of the beam
+            from oracle import ref_restated as rr
+            k = phase_first["rays"]
+            ref = rr.trace_rays(ogrid, rays_host[:, :k], dtau=sched.dtau, first_save=sched.first_save,
+                                save_every=1, n_saves=1, project=True, plane=L / 2,
+                                phase_mode="reference")["phase"][-1]
+            dens = rr.trace_rays(ogrid, rays_host[:, :k], dtau=sched.dtau, first_save=sched.first_save,
+                                 save_every=1, n_saves=1, project=True, plane=L / 2,
+                                 phase_mode="density")["phase"][-1]
+            sc = float(np.abs(ref).max())
+            phase_ref = {"rays": k, "oracle": "numpy FP64, phase_mode 'reference' (interpolated n - 1)",
+                         "fp64_port_rel_max": float(np.abs(phase_first["f64"] - ref).max() / sc),
+                         "fp32_rel_max": float(np.abs(phase_first["f32"] - ref).max() / sc),
+                         "density_form_gap_rel_max": float(np.abs(dens - ref).max() / sc)}
+        del ogrid
 
     if rank == 0:
         hbm_peak, peak_kind = measured_peaks()
@@ -643,7 +667,8 @@ def run_sloth(args):
                                        "samples the field 3 times (RK4 would sample it 4 times)",
                        "l2": f"inputs larger than L2 ({n ** 3 * 16 / 1e9:.2f} GB packed grid, "
                              f"{nrays * 24 / 1e6:.0f} MB rays)",
-                       "precision": "FP32 state with compensated sums, FP64 phase, Kahan FP32 optical depth",
+                       "precision": "FP32 state with compensated sums, FP64 phase accumulator, Kahan FP32 optical "
+                                    "depth; the phase integrand n - 1 is interpolated from the packed grid",
                        "seed": args.seed, "ray_steps_per_trace": ray_steps},
             "latency_ms": {"p50": float(np.percentile(per_step_ms, 50)), "p99": float(np.percentile(per_step_ms, 99)),
                            "what": "one 1e7-ray trace per request"},
@@ -671,6 +696,7 @@ def run_sloth(args):
             "clocks": clocks,
             "fp64_port": fp64,
             "fp32_vs_fp64": acc,
+            "phase_vs_reference_semantics": phase_ref,
             "rk4": rk4,
             "serving": serve,
             "adjoint": adj,

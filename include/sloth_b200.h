@@ -87,7 +87,7 @@ typedef struct SlothTraceParams {
     double  ope_ratio2;       /* (omega_pe/omega)^2 per unit ne/nc (NRL constants)  */
     double  q_max;            /* upper bound of ne/nc over the grid, or 0 if unknown;
                                  a bound selects faster exact paths (sub-critical
-                                 kappa; series n - 1 when (omega_pe/omega)^2 <= 0.05) */
+                                 kappa)                                           */
     double  q_min;            /* lower bound of ne/nc over the grid (0 for a density
                                  known to be >= 0). With q_max it bounds the ray's
                                  acceleration. Runs of steps that the bound proves
@@ -145,6 +145,18 @@ int sloth_grid_pack_f32(const SlothGridDesc* g, const void* ne, int ne_is_f64,
                         double ne_scale, void* grid_out, void* stream);
 int sloth_grid_pack_f64(const SlothGridDesc* g, const void* ne, int ne_is_f64,
                         double ne_scale, void* grid_out, void* stream);
+/* The trace layout, which the tracers (K2/K3) and the request server read:
+ * as above, but channel 0 holds the refractive index minus one instead of
+ * q, n - 1 = sqrt(1 - x) - 1 with x = ope_ratio2 * q = (omega_pe/omega)^2,
+ * evaluated in FP64 as -x / (1 + sqrt(1 - x)) and -x where x > 1. The
+ * tracers interpolate it for the optical phase, as the legacy solver
+ * interpolates its n grid (src/legacy/full_solver.py:289, :342-345), and
+ * rebuild q at the cell corners for the inverse-bremsstrahlung rate.
+ * ope_ratio2 as in SlothTraceParams (> 0). */
+int sloth_grid_pack_trace_f32(const SlothGridDesc* g, const void* ne, int ne_is_f64, double ne_scale,
+                              double ope_ratio2, void* grid_out, void* stream);
+int sloth_grid_pack_trace_f64(const SlothGridDesc* g, const void* ne, int ne_is_f64, double ne_scale,
+                              double ope_ratio2, void* grid_out, void* stream);
 
 /* ---- K0: trilinear sample -----------------------------------------------
  * Replaces RegularGridInterpolator (src/core/interpolator.py:15-105) on the
@@ -163,6 +175,7 @@ int sloth_sample_f64(const SlothGridDesc* g, const void* grid, const double* poi
  * _f32: FP32 state with compensated (Neumaier) position and velocity sums,
  * FP32 float4 grid, FP64 phase accumulator, Kahan FP32 optical depth.
  * _f64: the same kernel with every quantity in FP64 and a double grid.
+ * grid: the trace layout (sloth_grid_pack_trace_f32 / _f64).
  * rays: (6, N) row-major, float (f32) or double (f64).
  * workspace: device scratch of at least sloth_trace_workspace_bytes(N) bytes,
  * 256-byte aligned; its contents need not be initialised. */

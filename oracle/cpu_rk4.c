@@ -10,10 +10,12 @@
  *                                                       dtau/dt = kappa(r)
  *   interpolator        src/core/interpolator.py:79-104 trilinear, fill 0 outside
  *                       (the uniform-grid form of searchsorted-1 clamped to [0, n-2])
- *   phase integrand     src/legacy/full_solver.py:271-274, :341-347  omega*(n - 1)
+ *   phase integrand     src/legacy/full_solver.py:271-274, :289, :341-347  omega*(n - 1),
+ *                       n - 1 interpolated from its grid values (fill 0 outside, i.e. n = 1)
  *   keep_current_plane  src/shared/propagation.py:4-90
- * The grid fields (ne and the three gradient grids of G, kappa) come from the
- * numpy restatement of precompute_gradients / kappa_inv_brems, in SI units.
+ * The grid fields (ne and the three gradient grids of G, kappa, n - 1) come
+ * from the numpy restatement of precompute_gradients / kappa_inv_brems /
+ * n_refrac, in SI units.
  * Same semantics as trace_rays() in ref_restated.py, written independently
  * in C for speed (pthreads over rays, 64-ray chunks from an atomic counter).
  */
@@ -43,11 +45,12 @@ typedef struct {
     double plane;
     int32_t integrator;     /* 0: Runge-Kutta-Nystrom (3 samples), 1: classical RK4 (4 samples) */
     int32_t pad2;
+    const double* nm1;      /* (nx,ny,nz) n - 1 of the plasma refractive index */
 } OracleParams;
 
 typedef struct {
     double f[4];
-    double k;
+    double k, m;            /* kappa, n - 1 */
 } Samp;
 
 /* clip != 0 clamps the point into the grid in cell units first: a clamp in
@@ -85,14 +88,8 @@ static void sample(const OracleParams* p, const double r[3], int clip, Samp* s) 
                 s->f[2] += f[2] * w;
                 s->f[3] += f[3] * w;
                 if (p->kappa) s->k += p->kappa[v] * w;
+                s->m += p->nm1[v] * w;
             }
-}
-
-/* omega*(n - 1) with n = sqrt(1 - (omega_pe/omega)^2), omega_pe = 5.64e4*sqrt(ne_cc) */
-static double phase_rate(double ne, double omega) {
-    const double x = (5.64e4 * 5.64e4) * 1e-6 * ne / (omega * omega);
-    const double om = 1.0 - x > 0.0 ? 1.0 - x : 0.0;
-    return -omega * x / (1.0 + sqrt(om));
 }
 
 static void rhs(const OracleParams* p, const double r[3], int clip, double a[3], double* g, double* k) {
@@ -101,7 +98,7 @@ static void rhs(const OracleParams* p, const double r[3], int clip, double a[3],
     a[0] = s.f[1];
     a[1] = s.f[2];
     a[2] = s.f[3];
-    *g = phase_rate(s.f[0], p->omega);
+    *g = p->omega * s.m;   /* omega * (interpolated n - 1), 0 outside */
     *k = p->inv_brems ? s.k : 0.0;
 }
 

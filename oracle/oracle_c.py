@@ -23,7 +23,8 @@ class OracleParams(Structure):
                 ("fields", c_void_p), ("kappa", c_void_p), ("omega", c_double), ("dt", c_double),
                 ("first_save", c_int32), ("save_every", c_int32), ("n_saves", c_int32),
                 ("axis", c_int32), ("project", c_int32), ("inv_brems", c_int32), ("early_exit", c_int32),
-                ("threads", c_int32), ("plane", c_double), ("integrator", c_int32), ("pad2", c_int32)]
+                ("threads", c_int32), ("plane", c_double), ("integrator", c_int32), ("pad2", c_int32),
+                ("nm1", c_void_p)]
 
 
 _lib = None
@@ -54,8 +55,9 @@ def threads() -> int:
 
 def trace_rays(grid: "rr.Grid", rays, *, dtau, first_save, save_every, n_saves, axis=2, project=False,
                plane=0.0, inv_brems=False, early_exit=True, threads=0, want_state=True, integrator="rkn"):
-    """C version of ref_restated.trace_rays (phase_mode 'kernel'); integrator
-    'rkn' (Runge-Kutta-Nystrom, 3 samples) or 'rk4' (classical RK4, 4)."""
+    """C version of ref_restated.trace_rays (phase_mode 'reference': the
+    interpolated n - 1 grid); integrator 'rkn' (Runge-Kutta-Nystrom, 3
+    samples) or 'rk4' (classical RK4, 4)."""
     lib = load()
     rays = np.ascontiguousarray(rays, dtype=np.float64)
     n = rays.shape[1]
@@ -69,6 +71,8 @@ def trace_rays(grid: "rr.Grid", rays, *, dtau, first_save, save_every, n_saves, 
         p.origin[a] = grid.origin[a]
         p.spacing[a] = grid.spacing[a]
     p.fields = fields.ctypes.data
+    nm1 = np.ascontiguousarray(grid.nm1, dtype=np.float64)
+    p.nm1 = nm1.ctypes.data
     p.kappa = kappa.ctypes.data if kappa is not None else None
     p.omega = grid.omega
     p.dt = dtau / rr.C

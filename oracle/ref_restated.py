@@ -51,6 +51,12 @@ def n_refrac(ne, omega):
     return np.sqrt(1.0 - (omega_pe(ne * 1e-6) / omega) ** 2)
 
 
+def ope_ratio2(omega):
+    """(omega_pe/omega)^2 per unit ne/nc with the NRL omega_pe (5.64e4 rad/s per
+    sqrt(cm^-3), full_solver.py:236-239) and nc = ALPHA omega^2."""
+    return float((5.64e4 ** 2) * critical_density(omega) * 1e-6 / float(omega) ** 2)
+
+
 def critical_density(omega):
     """ncr = m_e eps0 omega^2 / e^2 in m^-3 (propagator.py:73)."""
     return ALPHA * float(omega) ** 2
@@ -98,13 +104,24 @@ def kappa_factors(Te, Z, omega):
 # ---------------------------------------------------------------------------
 # Kernel-layout grid (what K1 writes)
 # ---------------------------------------------------------------------------
-def pack_grid(ne, ne_scale):
-    """(nx, ny, nz, 4) float64: q = ne*ne_scale and dq per grid cell along
-    each axis, central inside and one-sided at the faces; the same formula as
-    the K1 kernel, in the same operation order."""
+def n_minus_1(x):
+    """n - 1 = sqrt(1 - x) - 1 of x = (omega_pe/omega)^2 as -x / (1 + sqrt(1 - x))
+    (no cancellation; equal to the legacy n_refrac - 1, full_solver.py:292-296,
+    to rounding), and -x above the critical density where the legacy n is
+    not real. Every operation is one IEEE rounding, as in the K1 kernel."""
+    x = np.asarray(x, dtype=np.float64)
+    return -(x / (1.0 + np.sqrt(np.maximum(1.0 - x, 0.0))))
+
+
+def pack_grid(ne, ne_scale, ope_ratio2=None):
+    """(nx, ny, nz, 4) float64: channel 0 and dq per grid cell along each axis,
+    central inside and one-sided at the faces, with q = ne*ne_scale; the same
+    formula as the K1 kernel, in the same operation order. Channel 0 is q
+    (the value layout) or, given ope_ratio2, n - 1 of x = ope_ratio2 * q
+    (the trace layout)."""
     q = np.asarray(ne, dtype=np.float64) * ne_scale
     out = np.empty(q.shape + (4,), dtype=np.float64)
-    out[..., 0] = q
+    out[..., 0] = q if ope_ratio2 is None else n_minus_1(ope_ratio2 * q)
     for ax in range(3):
         d = np.empty_like(q)
         sl = [slice(None)] * 3
@@ -227,7 +244,7 @@ class Grid:
         grads = precompute_gradients(self.ne, *coords, omega)
         self.fields = np.stack([self.ne, *grads], axis=-1)       # (nx,ny,nz,4)
         self.kappa = None if Te is None else kappa_inv_brems(self.ne, Te, Z, omega)
-        self.nm1 = n_refrac(self.ne, omega) - 1.0
+        self.nm1 = n_minus_1((omega_pe(self.ne * 1e-6) / self.omega) ** 2)
 
     def sample(self, r, *, with_kappa=False, with_nm1=False, clip=None):
         """Interpolate the four fields (and kappa / n-1) at r (3, N); 0 outside.
@@ -276,7 +293,7 @@ def phase_integrand(ne_interp, omega, nc):
 
 def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=2,
                project=False, plane=0.0, inv_brems=False, early_exit=True,
-               phase_mode="kernel", integrator="rkn"):
+               phase_mode="reference", integrator="rkn"):
     """Fixed-step fourth-order Runge-Kutta-Nystrom integration of dsdt
     (+ phase, + optical depth) in SI units: three samples per step,
     r2 = r + h/2 v + h^2/8 a1, r3 = r + h v + h^2/2 a2, r' = r + h v +
@@ -295,8 +312,9 @@ def trace_rays(grid: Grid, rays, *, dtau, first_save, save_every, n_saves, axis=
     step whose prediction ends within FACE_MARGIN cells of a face, samples its
     stage points clamped into the grid box: it integrates the field's limit
     from inside, as an event-locating adaptive solver does. kappa is the reference's interpolated kappa
-    grid; phase_mode 'kernel' takes n from the interpolated density,
-    'reference' interpolates the (n - 1) grid (full_solver.py:289).
+    grid; phase_mode 'reference' (the tracers' semantics) interpolates the
+    (n - 1) grid as the legacy solver interpolates n (full_solver.py:289),
+    'density' takes n from the interpolated density instead.
     integrator 'rk4' takes classical RK4 steps of the first-order system
     instead (four samples, RK4's weights (1, 2, 2, 1)/6 for the integrals).
     Returns a dict of arrays.

@@ -130,6 +130,10 @@ _SIGNATURES = {
     "sloth_grid_bytes": (c_size_t, [POINTER(SlothGridDesc), c_int]),
     "sloth_grid_pack_f32": (c_int, [POINTER(SlothGridDesc), c_void_p, c_int, c_double, c_void_p, c_void_p]),
     "sloth_grid_pack_f64": (c_int, [POINTER(SlothGridDesc), c_void_p, c_int, c_double, c_void_p, c_void_p]),
+    "sloth_grid_pack_trace_f32": (c_int, [POINTER(SlothGridDesc), c_void_p, c_int, c_double, c_double, c_void_p,
+                                          c_void_p]),
+    "sloth_grid_pack_trace_f64": (c_int, [POINTER(SlothGridDesc), c_void_p, c_int, c_double, c_double, c_void_p,
+                                          c_void_p]),
     "sloth_sample_f32": (c_int, [POINTER(SlothGridDesc), c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
     "sloth_sample_f64": (c_int, [POINTER(SlothGridDesc), c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
     "sloth_trace_workspace_bytes": (c_size_t, [c_int64]),

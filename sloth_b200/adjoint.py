@@ -81,7 +81,8 @@ def _image_forward(ne: torch.Tensor, rays: torch.Tensor, origin, spacing, omega:
     rays = rays.to(dt).contiguous()
     if rays.dim() != 2 or rays.shape[0] != 6:
         raise ValueError("rays must be (6, N)")
-    grid = runtime.pack_grid(ne.detach(), origin, spacing, omega, precision=precision, device=ne.device)
+    grid = runtime.pack_grid(ne.detach(), origin, spacing, omega, precision=precision, device=ne.device,
+                             layout="values")
     params = spec.params()
     n = int(rays.shape[1])
     ws_bytes = int(capi.load().sloth_image_workspace_bytes(ctypes.byref(params), n))

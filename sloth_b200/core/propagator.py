@@ -102,7 +102,7 @@ def precompute_gradients(ne, x, y, z, omega, *, device=None):
     _check_overcritical(ne, omega)
     origin, spacing, _ = zip(*(runtime.uniform_axis(a) for a in (x, y, z)))
     g = runtime.pack_grid(ne if isinstance(ne, torch.Tensor) else np.asarray(ne), origin, spacing, omega,
-                          precision="f64", device=device)
+                          precision="f64", device=device, layout="values")
     n = g.n
     v = g.data.view(*n, 4).cpu().numpy()
     return tuple(-0.5 * C ** 2 * v[..., 1 + a] / spacing[a] for a in range(3))
@@ -117,7 +117,7 @@ def dndr(r, dndx, dndy, dndz, x, y, z):
     for d in (dndx, dndy, dndz):
         # the gradient grid becomes the q channel of a unit-scale packed grid
         g = runtime.pack_grid(np.asarray(d, dtype=np.float64), origin, spacing, 1.0, precision="f64",
-                              ne_scale=1.0)
+                              ne_scale=1.0, layout="values")
         out.append(runtime.sample(g, r.T)[0].cpu().numpy())
     return np.stack(out)
 
@@ -135,7 +135,7 @@ def dsdt(t, s, parallelise, dndx, dndy, dndz, x, y, z, lengths, dims, kappa=None
     if kappa is not None:
         origin, spacing, _ = zip(*(runtime.uniform_axis(a) for a in (x, y, z)))
         g = runtime.pack_grid(np.asarray(kappa, dtype=np.float64), origin, spacing, 1.0, precision="f64",
-                              ne_scale=1.0)
+                              ne_scale=1.0, layout="values")
         sprime[6] = runtime.sample(g, r.T)[0].cpu().numpy()
     return np.ravel(sprime)
 

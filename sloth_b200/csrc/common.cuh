@@ -1,9 +1,10 @@
 // Shared device code of the sloth_b200 library (sm_100a).
 //
 // Grid layout: one 16-byte voxel per grid point holding
-//   (q, dq/du, dq/dv, dq/dw),  q = ne/nc,  d/du = derivative per grid cell,
-// in C order (z fastest). The FP64 port stores the same four values as two
-// double2 (32 bytes per voxel).
+//   (c0, dq/du, dq/dv, dq/dw),  q = ne/nc,  d/du = derivative per grid cell,
+// in C order (z fastest), with c0 = q (the value layout) or c0 = n - 1, the
+// plasma refractive index minus one (the trace layout the tracers read). The
+// FP64 port stores the same four values as two double2 (32 bytes per voxel).
 //
 // Ray coordinates inside the tracers are in grid cells (p = (x - x0)/h) and
 // the velocity in cells per step (w = (v/c) * dtau / h), so one integration step is a
@@ -111,13 +112,6 @@ struct PolF32 {
         const float4 v = __ldg(reinterpret_cast<const float4*>(g) + i);
         return V{v.x, v.y, v.z, v.w};
     }
-    // n - 1 for the plasma refractive index n = sqrt(1 - q), written as
-    // -q / (1 + sqrt(1 - q)) to avoid cancellation; 0 for q <= 0.
-    __device__ __forceinline__ static float n_minus_1(float q) {
-        const float om = fmaxf(1.0f - q, 0.0f);
-        const float s = om > 0.0f ? om * rsqrtf(om) : 0.0f;
-        return -__fdividef(q, 1.0f + s);
-    }
     __device__ __forceinline__ static float log_(float x) { return __logf(x); }
 };
 
@@ -131,10 +125,6 @@ struct PolF64 {
         const double2* p = reinterpret_cast<const double2*>(g) + 2u * (size_t)i;
         const double2 a = __ldg(p), b = __ldg(p + 1);
         return V{a.x, a.y, b.x, b.y};
-    }
-    __device__ __forceinline__ static double n_minus_1(double q) {
-        const double om = fmax(1.0 - q, 0.0);
-        return -q / (1.0 + sqrt(om));
     }
     __device__ __forceinline__ static double log_(double x) { return log(x); }
 };

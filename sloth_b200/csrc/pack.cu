@@ -6,6 +6,13 @@
 // first-order one-sided differences on the two faces). Here the gradient is
 // kept per grid cell and normalised to the critical density, q = ne/nc; the
 // tracers fold the -c^2/2 and 1/h^2 factors into one per-axis constant.
+// Channel 0 holds q itself (the value layout, read by the K0 sampler and the
+// detector-image model) or, in the trace layout, the refractive index minus
+// one, n - 1 = sqrt(1 - x) - 1 with x = (omega_pe/omega)^2 = ope_ratio2 * q,
+// which the tracers interpolate for the optical phase as the legacy solver
+// interpolates its n grid (src/legacy/full_solver.py:289, :292-296, :342-345).
+// It is evaluated as -x / (1 + sqrt(1 - x)), free of cancellation, and is -x
+// above the critical density (where the legacy n is not real).
 // All arithmetic is FP64; the FP32 grid rounds the final values once.
 #include "common.cuh"
 
@@ -22,9 +29,17 @@ __device__ __forceinline__ double qat(const In* __restrict__ ne, size_t i, doubl
 // Launch shape: x over k (contiguous, coalesced), y over j, z over i, each
 // axis strided when the grid has more points than the launch dimension; no
 // index arithmetic beyond a multiply-add per voxel.
-template <class In, bool F64OUT>
+// n - 1 of x = ope2 * q, every operation rounded on its own (no fused
+// multiply-add), so that it equals a plain IEEE evaluation of the formula.
+__device__ __forceinline__ double n_minus_1_of(double q, double ope2) {
+    const double x = __dmul_rn(ope2, q);
+    const double om = fmax(__dsub_rn(1.0, x), 0.0);
+    return -__ddiv_rn(x, __dadd_rn(1.0, __dsqrt_rn(om)));
+}
+
+template <class In, bool F64OUT, bool NM1>
 __global__ void __launch_bounds__(256) pack_kernel(const In* __restrict__ ne, void* __restrict__ out,
-                                                   GridGeo g, double scale) {
+                                                   GridGeo g, double scale, double ope2) {
   for (int i = blockIdx.z; i < g.n[0]; i += gridDim.z)
     for (int j = blockIdx.y; j < g.n[1]; j += gridDim.y)
       for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.n[2]; k += gridDim.x * blockDim.x) {
@@ -40,12 +55,13 @@ __global__ void __launch_bounds__(256) pack_kernel(const In* __restrict__ ne, vo
         if (k == 0)               d2 = qat(ne, vi + 1, scale) - q;
         else if (k == g.n[2] - 1) d2 = q - qat(ne, vi - 1, scale);
         else                      d2 = 0.5 * (qat(ne, vi + 1, scale) - qat(ne, vi - 1, scale));
+        const double c0 = NM1 ? n_minus_1_of(q, ope2) : q;
         if (F64OUT) {
             double2* o = reinterpret_cast<double2*>(out) + 2 * vi;
-            o[0] = make_double2(q, d0);
+            o[0] = make_double2(c0, d0);
             o[1] = make_double2(d1, d2);
         } else {
-            reinterpret_cast<float4*>(out)[vi] = make_float4((float)q, (float)d0, (float)d1, (float)d2);
+            reinterpret_cast<float4*>(out)[vi] = make_float4((float)c0, (float)d0, (float)d1, (float)d2);
         }
       }
 }
@@ -87,13 +103,14 @@ static int grid_blocks(long long work, int per_sm) {
     return (int)b;
 }
 
-template <bool F64OUT>
-static int pack_impl(const SlothGridDesc* g, const void* ne, int ne_is_f64, double ne_scale,
+template <bool F64OUT, bool NM1>
+static int pack_impl(const SlothGridDesc* g, const void* ne, int ne_is_f64, double ne_scale, double ope2,
                      void* grid_out, void* stream) {
     int rc = check_grid(g);
     if (rc) return rc;
     if (!ne || !grid_out) return SLOTH_ERR_NULL_POINTER;
     if (!(ne_scale > 0.0) || !std::isfinite(ne_scale)) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (NM1 && (!(ope2 > 0.0) || !std::isfinite(ope2))) return SLOTH_ERR_INVALID_ARGUMENT;
     if (((uintptr_t)grid_out & 15u) != 0) return SLOTH_ERR_MISALIGNED;
     if (((uintptr_t)ne & (ne_is_f64 ? 7u : 3u)) != 0) return SLOTH_ERR_MISALIGNED;
     const GridGeo geo = make_geo(g);
@@ -102,9 +119,9 @@ static int pack_impl(const SlothGridDesc* g, const void* ne, int ne_is_f64, doub
     (void)total;
     const dim3 grid = voxel_grid(g);
     if (ne_is_f64)
-        pack_kernel<double, F64OUT><<<grid, 256, 0, s>>>((const double*)ne, grid_out, geo, ne_scale);
+        pack_kernel<double, F64OUT, NM1><<<grid, 256, 0, s>>>((const double*)ne, grid_out, geo, ne_scale, ope2);
     else
-        pack_kernel<float, F64OUT><<<grid, 256, 0, s>>>((const float*)ne, grid_out, geo, ne_scale);
+        pack_kernel<float, F64OUT, NM1><<<grid, 256, 0, s>>>((const float*)ne, grid_out, geo, ne_scale, ope2);
     note_launch();
     return cuda_status(cudaGetLastError());
 }
@@ -139,12 +156,22 @@ size_t sloth_grid_bytes(const SlothGridDesc* g, int real_bytes) {
 
 int sloth_grid_pack_f32(const SlothGridDesc* g, const void* ne, int ne_is_f64, double ne_scale,
                         void* grid_out, void* stream) {
-    return sloth::pack_impl<false>(g, ne, ne_is_f64, ne_scale, grid_out, stream);
+    return sloth::pack_impl<false, false>(g, ne, ne_is_f64, ne_scale, 0.0, grid_out, stream);
 }
 
 int sloth_grid_pack_f64(const SlothGridDesc* g, const void* ne, int ne_is_f64, double ne_scale,
                         void* grid_out, void* stream) {
-    return sloth::pack_impl<true>(g, ne, ne_is_f64, ne_scale, grid_out, stream);
+    return sloth::pack_impl<true, false>(g, ne, ne_is_f64, ne_scale, 0.0, grid_out, stream);
+}
+
+int sloth_grid_pack_trace_f32(const SlothGridDesc* g, const void* ne, int ne_is_f64, double ne_scale,
+                              double ope_ratio2, void* grid_out, void* stream) {
+    return sloth::pack_impl<false, true>(g, ne, ne_is_f64, ne_scale, ope_ratio2, grid_out, stream);
+}
+
+int sloth_grid_pack_trace_f64(const SlothGridDesc* g, const void* ne, int ne_is_f64, double ne_scale,
+                              double ope_ratio2, void* grid_out, void* stream) {
+    return sloth::pack_impl<true, true>(g, ne, ne_is_f64, ne_scale, ope_ratio2, grid_out, stream);
 }
 
 int sloth_sample_f32(const SlothGridDesc* g, const void* grid, const double* points, int64_t n,

@@ -38,9 +38,7 @@
 
 namespace sloth {
 
-constexpr int kModes = 5;   // (IB_OFF, x), (IB_OFF, smallx), (SUB, x), (SUB, smallx), (GENERAL, x)
-
-inline int mode_index(int ib, bool smallx) { return ib == IB_GENERAL ? 4 : ib * 2 + (smallx ? 1 : 0); }
+constexpr int kModes = 3;   // the inverse-bremsstrahlung paths IB_OFF, IB_SUBCRITICAL, IB_GENERAL
 
 struct WorkItem {
     int slot;
@@ -54,7 +52,7 @@ struct WorkHeader {
     int pad;
 };
 
-template <int IB, bool SMALLX>
+template <int IB>
 __global__ void __launch_bounds__(kThreads, SLOTH_TRACE_MIN_BLOCKS)
 serve_kernel(const TraceArgs* __restrict__ table, WorkHeader* hdr, const WorkItem* __restrict__ items, int mode) {
     __shared__ TraceArgs s_args;
@@ -98,9 +96,9 @@ serve_kernel(const TraceArgs* __restrict__ table, WorkHeader* hdr, const WorkIte
         unsigned long long my_steps = 0;
         // the job's density range bounds its accelerations: the interior fast path
         if (interior_sampling_ok(s_args))
-            trace_tile<PolF32, IB, SMALLX, 1>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
+            trace_tile<PolF32, IB, 1>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
         else
-            trace_tile<PolF32, IB, SMALLX, 0>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
+            trace_tile<PolF32, IB, 0>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
         block_add(my_steps, &s_steps, s_args.total_steps);
     }
 }
@@ -269,7 +267,7 @@ static size_t job_bytes(long long n, const SlothTraceParams* p, int* bbits_out, 
 }
 
 static int graph_build(ServerImpl* s, IterSlot& is, int blocks[kModes]) {
-    // captured once per iteration slot: work list H2D, then the five mode
+    // captured once per iteration slot: work list H2D, then the three mode
     // kernels on parallel branches joined back into the slot's stream
     cudaStream_t side[kModes];
     cudaEvent_t fork = nullptr, join[kModes];
@@ -288,11 +286,9 @@ static int graph_build(ServerImpl* s, IterSlot& is, int blocks[kModes]) {
         for (int m = 0; m < kModes; ++m) {
             cudaStreamWaitEvent(side[m], fork, 0);
             switch (m) {
-                case 0: serve_kernel<IB_OFF, false><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
-                case 1: serve_kernel<IB_OFF, true><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
-                case 2: serve_kernel<IB_SUBCRITICAL, false><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
-                case 3: serve_kernel<IB_SUBCRITICAL, true><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
-                default: serve_kernel<IB_GENERAL, false><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
+                case IB_OFF: serve_kernel<IB_OFF><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
+                case IB_SUBCRITICAL: serve_kernel<IB_SUBCRITICAL><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
+                default: serve_kernel<IB_GENERAL><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
             }
             cudaEventRecord(join[m], side[m]);
             cudaStreamWaitEvent(is.stream, join[m], 0);
@@ -309,10 +305,10 @@ static int graph_build(ServerImpl* s, IterSlot& is, int blocks[kModes]) {
     return cuda_status(e);
 }
 
-template <int IB, bool SMALLX>
+template <int IB>
 static int resident_blocks(int sms) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, serve_kernel<IB, SMALLX>, kThreads, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, serve_kernel<IB>, kThreads, 0) != cudaSuccess ||
         b < 1)
         b = 1;
     return b * sms;
@@ -364,7 +360,8 @@ static int admit_one(ServerImpl* s, Job& j) {
         g.off = goff;
         g.bytes = gb;
         const double nc = 3.14207787e-4 * j.p.omega * j.p.omega;
-        int rc = sloth_grid_pack_f32(&j.desc, j.ne, j.ne_is_f64, 1.0 / nc, s->arena.ptr(goff), s->admit);
+        int rc = sloth_grid_pack_trace_f32(&j.desc, j.ne, j.ne_is_f64, 1.0 / nc, j.p.ope_ratio2, s->arena.ptr(goff),
+                                           s->admit);
         if (rc) {
             s->arena.release(goff, gb);
             return rc;
@@ -417,10 +414,7 @@ static int admit_one(ServerImpl* s, Job& j) {
     fill_trace_args(ta, &ge->desc, s->arena.ptr(ge->off), &j.p, rays, j.n, &j.out, perm, skeys);
     e = cudaMemcpyAsync(s->d_table + j.slot, &ta, sizeof(TraceArgs), cudaMemcpyHostToDevice, s->admit);
     if (e != cudaSuccess) return cuda_status(e);
-    int ib;
-    bool smallx;
-    trace_mode(&j.p, &ib, &smallx);
-    j.mode = mode_index(ib, smallx);
+    j.mode = trace_mode(&j.p);
     j.tiles_total = (int)((j.n + kTile - 1) / kTile);
     j.tiles_assigned = 0;
     j.state = JOB_ADMITTED;
@@ -631,11 +625,9 @@ int sloth_server_create(const SlothServerConfig* cfg, SlothServer** out) {
         (e = cudaEventCreate(&s->t0)) != cudaSuccess || (e = cudaEventRecord(s->t0, s->admit)) != cudaSuccess)
         return fail(sloth::cuda_status(e));
     for (int i = cfg->max_jobs - 1; i >= 0; --i) s->free_slots.push_back(i);
-    int blocks[sloth::kModes] = {sloth::resident_blocks<sloth::IB_OFF, false>(s->sms),
-                                 sloth::resident_blocks<sloth::IB_OFF, true>(s->sms),
-                                 sloth::resident_blocks<sloth::IB_SUBCRITICAL, false>(s->sms),
-                                 sloth::resident_blocks<sloth::IB_SUBCRITICAL, true>(s->sms),
-                                 sloth::resident_blocks<sloth::IB_GENERAL, false>(s->sms)};
+    int blocks[sloth::kModes] = {sloth::resident_blocks<sloth::IB_OFF>(s->sms),
+                                 sloth::resident_blocks<sloth::IB_SUBCRITICAL>(s->sms),
+                                 sloth::resident_blocks<sloth::IB_GENERAL>(s->sms)};
     const size_t wbytes = sizeof(sloth::WorkHeader) + sizeof(sloth::WorkItem) * (size_t)cfg->tiles_per_step;
     for (auto& is : s->it) {
         if ((e = cudaStreamCreateWithFlags(&is.stream, cudaStreamNonBlocking)) != cudaSuccess ||

@@ -6,7 +6,7 @@
 
 namespace sloth {
 
-template <class P, int IB, bool SMALLX, int FAST, int INTEG>
+template <class P, int IB, int FAST, int INTEG>
 __global__ void __launch_bounds__(kThreads, SLOTH_TRACE_MIN_BLOCKS)
 trace_kernel(const __grid_constant__ TraceArgs a) {
     __shared__ unsigned s_key[kTile];
@@ -38,13 +38,13 @@ trace_kernel(const __grid_constant__ TraceArgs a) {
             start = (long long)a.n_big * kTile + (long long)(tile - a.n_big) * kSmallTile;
             cnt = (int)min((long long)kSmallTile, a.n - start);
         }
-        trace_tile<P, IB, SMALLX, FAST, INTEG>(a, start, cnt, s_key, s_id, &s_head, cc, my_steps);
+        trace_tile<P, IB, FAST, INTEG>(a, start, cnt, s_key, s_id, &s_head, cc, my_steps);
     }
     // one atomic per CTA for the ray-step total
     block_add(my_steps, &s_steps, a.total_steps);
 }
 
-template <class P, int IB, bool SMALLX, int FAST, int INTEG>
+template <class P, int IB, int FAST, int INTEG>
 static int launch_trace_k(const TraceArgs& ta, int sms, cudaStream_t s) {
     static int cached[64] = {0};
     int dev = 0;
@@ -52,7 +52,7 @@ static int launch_trace_k(const TraceArgs& ta, int sms, cudaStream_t s) {
     if (e != cudaSuccess) return cuda_status(e);
     int per_sm = (dev >= 0 && dev < 64) ? cached[dev] : 0;
     if (per_sm <= 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel<P, IB, SMALLX, FAST, INTEG>, kThreads, 0) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel<P, IB, FAST, INTEG>, kThreads, 0) !=
                 cudaSuccess || per_sm < 1)
             per_sm = 1;
         if (dev >= 0 && dev < 64) cached[dev] = per_sm;
@@ -65,22 +65,22 @@ static int launch_trace_k(const TraceArgs& ta, int sms, cudaStream_t s) {
     const long long rest = ta.n - (long long)t.n_big * kTile;
     t.n_tiles = t.n_big + (int)((rest + kSmallTile - 1) / kSmallTile);
     if (blocks > t.n_tiles) blocks = t.n_tiles;
-    trace_kernel<P, IB, SMALLX, FAST, INTEG><<<(int)blocks, kThreads, 0, s>>>(t);
+    trace_kernel<P, IB, FAST, INTEG><<<(int)blocks, kThreads, 0, s>>>(t);
     note_launch();
     return cuda_status(cudaGetLastError());
 }
 
-template <class P, int IB, bool SMALLX, int INTEG>
+template <class P, int IB, int INTEG>
 static int launch_trace_i(const TraceArgs& ta, int sms, cudaStream_t s, int fast) {
-    return fast == 1 ? launch_trace_k<P, IB, SMALLX, 1, INTEG>(ta, sms, s)
-         : fast == 2 ? launch_trace_k<P, IB, SMALLX, 2, INTEG>(ta, sms, s)
-                     : launch_trace_k<P, IB, SMALLX, 0, INTEG>(ta, sms, s);
+    return fast == 1 ? launch_trace_k<P, IB, 1, INTEG>(ta, sms, s)
+         : fast == 2 ? launch_trace_k<P, IB, 2, INTEG>(ta, sms, s)
+                     : launch_trace_k<P, IB, 0, INTEG>(ta, sms, s);
 }
 
-template <class P, int IB, bool SMALLX>
+template <class P, int IB>
 static int launch_trace(const TraceArgs& ta, int sms, cudaStream_t s, int fast, int integ) {
-    return integ == INTEG_RK4 ? launch_trace_i<P, IB, SMALLX, INTEG_RK4>(ta, sms, s, fast)
-                              : launch_trace_i<P, IB, SMALLX, INTEG_RKN>(ta, sms, s, fast);
+    return integ == INTEG_RK4 ? launch_trace_i<P, IB, INTEG_RK4>(ta, sms, s, fast)
+                              : launch_trace_i<P, IB, INTEG_RKN>(ta, sms, s, fast);
 }
 
 template <class P>
@@ -130,9 +130,7 @@ static int trace_impl(const SlothGridDesc* g, const void* grid, const SlothTrace
     TraceArgs ta;
     fill_trace_args(ta, g, grid, p, rays, n, out, perm, skeys);
     ta.tile_counter = tile_counter;
-    int ib;
-    bool smallx;
-    trace_mode(p, &ib, &smallx);
+    const int ib = trace_mode(p);
     // interior runs with interior sampling, interior runs only, or neither
     const int fast = interior_bound_ok(g, p) ? 1 : (std::isfinite(interior_accel_bound(g, p)) ? 2 : 0);
 
@@ -142,13 +140,11 @@ static int trace_impl(const SlothGridDesc* g, const void* grid, const SlothTrace
     }
     const int integ = p->integrator;
     if (ib == IB_OFF)
-        rc = smallx ? launch_trace<P, IB_OFF, true>(ta, sms, s, fast, integ)
-                    : launch_trace<P, IB_OFF, false>(ta, sms, s, fast, integ);
+        rc = launch_trace<P, IB_OFF>(ta, sms, s, fast, integ);
     else if (ib == IB_SUBCRITICAL)
-        rc = smallx ? launch_trace<P, IB_SUBCRITICAL, true>(ta, sms, s, fast, integ)
-                    : launch_trace<P, IB_SUBCRITICAL, false>(ta, sms, s, fast, integ);
+        rc = launch_trace<P, IB_SUBCRITICAL>(ta, sms, s, fast, integ);
     else
-        rc = launch_trace<P, IB_GENERAL, false>(ta, sms, s, fast, integ);
+        rc = launch_trace<P, IB_GENERAL>(ta, sms, s, fast, integ);
     if (rc) return rc;
     if (out->trace_event_end) {
         e = cudaEventRecord((cudaEvent_t)out->trace_event_end, s);

@@ -11,8 +11,9 @@
 //                    ray_to_Jonesvector (src/shared/propagation.py:4-90).
 // What runs here: the same ODE with a fixed-step fourth-order Runge-Kutta-
 // Nystrom method in scaled units (grid cells, cells per step; see rkn_step),
-// one thread per ray, plus the optical phase integral of omega*(n - 1)
-// (src/legacy/full_solver.py:341-347, n = sqrt(1 - ne/nc)) and the
+// one thread per ray, plus the optical phase integral of omega*(n - 1) with
+// n - 1 interpolated from the trace layout's channel 0, as the legacy solver
+// interpolates its n grid (src/legacy/full_solver.py:289, :341-347), and the
 // inverse-bremsstrahlung optical depth, both as Simpson quadratures of the
 // stage values, and the Jones-vector projection at each save.
 //
@@ -56,7 +57,6 @@ namespace sloth {
 
 constexpr int kThreads = SLOTH_TRACE_THREADS;
 constexpr double kFaceMargin = 0.02;     // cells
-constexpr double kSmallX = 0.05;         // bound on (omega_pe/omega)^2 for the series form of n - 1
 
 // Inverse-bremsstrahlung modes of the tracer.
 enum { IB_OFF = 0, IB_SUBCRITICAL = 1, IB_GENERAL = 2 };
@@ -101,12 +101,14 @@ struct TraceArgs {
     float Sf[3];               // the same, rounded to FP32 once here (the FP32 tracer reads these
                                // instead of converting the doubles inside its loop)
     float ope2f, cl_lof, cl_wf;
+    float inv_ope2f;           // 1 / ope2 (q from x = ope2 * q)
     float accel_bound;         // bound on |acceleration| (cells per step^2), 0 when unknown
                                // (see interior_run and interior_sampling_ok)
     double phase_scale;        // (omega/c) * dtau / 6
     double tau_scale;          // kappa_q2 * dtau / 6
     double cl_w, cl_lo;        // Coulomb log below nc, and max(2, cl_w)
     double ope2;               // (omega_pe/omega)^2 per unit q
+    double inv_ope2;
     double plane;
     int first_save, save_every, n_saves;
     int axis, t1, t2;
@@ -133,6 +135,9 @@ template <class R> __device__ __forceinline__ R arg_cl_lo(const TraceArgs& a) {
 template <class R> __device__ __forceinline__ R arg_cl_w(const TraceArgs& a) {
     if constexpr (sizeof(R) == 4) return a.cl_wf; else return a.cl_w;
 }
+template <class R> __device__ __forceinline__ R arg_inv_ope2(const TraceArgs& a) {
+    if constexpr (sizeof(R) == 4) return a.inv_ope2f; else return a.inv_ope2;
+}
 
 __device__ __forceinline__ double sel3(const double (&v)[3], int i) {
     return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]);
@@ -157,9 +162,11 @@ struct CellCache {
     typename P::V c[8];
 };
 
+// One field sample: n - 1 (the trace layout's channel 0), the three gradient
+// channels and the inverse-bremsstrahlung rate per kappa_q2.
 template <class P>
 struct Sample {
-    typename P::R q, g0, g1, g2, k;
+    typename P::R n1, g0, g1, g2, k;
 };
 
 // A cached cell as trilinear polynomials in the in-cell coordinates
@@ -251,47 +258,36 @@ __device__ __forceinline__ float2 poly_eval2(const float2 (&t)[8], float2 fx, fl
 template <class C> struct IsPairedCache : std::false_type {};
 template <int NK> struct IsPairedCache<CellPolyF2<NK>> : std::true_type {};
 
-// n - 1 for n = sqrt(1 - x), x = (omega_pe/omega)^2. SMALLX (FP32 only, used
-// when x <= kSmallX over the whole grid) takes the binomial series
-// -(x/2 + x^2/8 + x^3/16 + 5x^4/128 + 7x^5/256), whose first omitted term is
-// below 2e-8 of x/2 there, instead of a square root and a division.
-template <class P, bool SMALLX>
-__device__ __forceinline__ typename P::R nm1(typename P::R x) {
-    using R = typename P::R;
-    if constexpr (SMALLX && sizeof(R) == 4) {
-        return -x * (R(0.5) + x * (R(0.125) + x * (R(0.0625) + x * (R(0.0390625) + x * R(0.02734375)))));
-    } else {
-        return P::n_minus_1(x);
-    }
-}
-
-// The FP32 series of nm1 for two arguments at once (sm_100 paired FP32).
-__device__ __forceinline__ float2 nm1_series2(float2 x) {
-    const float2 c = make_float2(0.02734375f, 0.02734375f);
-    float2 t = __ffma2_rn(x, c, make_float2(0.0390625f, 0.0390625f));
-    t = __ffma2_rn(x, t, make_float2(0.0625f, 0.0625f));
-    t = __ffma2_rn(x, t, make_float2(0.125f, 0.125f));
-    t = __ffma2_rn(x, t, make_float2(0.5f, 0.5f));
-    return __fmul2_rn(make_float2(-x.x, -x.y), t);
-}
-
-// The same series for one argument, rounded exactly as each lane of the pair.
-__device__ __forceinline__ float nm1_series1(float x) {
-    float t = __fmaf_rn(x, 0.02734375f, 0.0390625f);
-    t = __fmaf_rn(x, t, 0.0625f);
-    t = __fmaf_rn(x, t, 0.125f);
-    t = __fmaf_rn(x, t, 0.5f);
-    return __fmul_rn(-x, t);
+// x = (omega_pe/omega)^2 of a grid point from its n - 1 (the trace layout):
+// n - 1 = sqrt(1 - x) - 1 gives x = -(n - 1)(2 + (n - 1)) up to the critical
+// density (n - 1 >= -1), and the layout stores -x above it.
+template <class R>
+__device__ __forceinline__ R x_of_n1(R n1) {
+    if constexpr (sizeof(R) == 4)
+        return n1 >= -1.0f ? -__fmul_rn(n1, __fadd_rn(2.0f, n1)) : -n1;
+    else
+        return n1 >= -1.0 ? -__dmul_rn(n1, __dadd_rn(2.0, n1)) : -n1;
 }
 
 // Inverse-bremsstrahlung rate of one grid point per kappa_q2: q^2 * CL(q),
-// CL = max(2, cl_w - ln(max(omega_pe/omega, 1))) (src/core/propagator.py:155-162).
+// CL = max(2, cl_w - ln(max(omega_pe/omega, 1))) (src/core/propagator.py:155-162),
+// with q rebuilt from the point's n - 1.
 template <class P>
-__device__ __forceinline__ typename P::R corner_kappa(const TraceArgs& a, typename P::R q) {
+__device__ __forceinline__ typename P::R corner_kappa(const TraceArgs& a, typename P::R n1) {
     using R = typename P::R;
-    const R x = q * arg_ope2<R>(a);
+    const R x = x_of_n1<R>(n1);
+    const R q = x * arg_inv_ope2<R>(a);
     const R cl = (x > R(1)) ? fmax(R(2), arg_cl_w<R>(a) - R(0.5) * P::log_(x)) : arg_cl_lo<R>(a);
     return q * q * cl;
+}
+
+// Below the critical density the rate is kappa_q2 * CL * q^2 with a constant
+// CL, so the sub-critical corners carry x^2 = (ope2 * q)^2 and the optical
+// depth's scale the constant factor cl_lo / ope2^2.
+template <class R>
+__device__ __forceinline__ R corner_x2(R n1) {
+    const R x = x_of_n1<R>(n1);
+    if constexpr (sizeof(R) == 4) return __fmul_rn(x, x); else return __dmul_rn(x, x);
 }
 
 // Loads cell b into the paired cache: its polynomial coefficients, two
@@ -315,8 +311,8 @@ __device__ __forceinline__ void paired_fill(const TraceArgs& a, unsigned b, Cell
 #undef SLOTH_HI
     if constexpr (IB == IB_SUBCRITICAL) {
         float k[8];
-        poly_coeffs<float>(k, v0.x * v0.x, v1.x * v1.x, v2.x * v2.x, v3.x * v3.x, v4.x * v4.x, v5.x * v5.x,
-                           v6.x * v6.x, v7.x * v7.x);
+        poly_coeffs<float>(k, corner_x2(v0.x), corner_x2(v1.x), corner_x2(v2.x), corner_x2(v3.x), corner_x2(v4.x),
+                           corner_x2(v5.x), corner_x2(v6.x), corner_x2(v7.x));
         kappa_store(k);
     } else if constexpr (IB == IB_GENERAL) {
         float k[8];
@@ -373,7 +369,7 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
         const bool in = (p[0] >= R(0)) & (p[0] <= lim_of<R>(g, 0)) & (p[1] >= R(0)) &
                         (p[1] <= lim_of<R>(g, 1)) & (p[2] >= R(0)) & (p[2] <= lim_of<R>(g, 2));
         if (!in) {
-            out.q = out.g0 = out.g1 = out.g2 = out.k = R(0);
+            out.n1 = out.g0 = out.g1 = out.g2 = out.k = R(0);
             return;
         }
         ix = min((int)p[0], g.n[0] - 2);
@@ -392,12 +388,12 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
         const float2 fx2 = make_float2(fx, fx), fy2 = make_float2(fy, fy), fz2 = make_float2(fz, fz);
         const float2 r0 = poly_eval2(cc.t[0], fx2, fy2, fz2);
         const float2 r1 = poly_eval2(cc.t[1], fx2, fy2, fz2);
-        out.q = r0.x;
+        out.n1 = r0.x;
         out.g0 = r0.y;
         out.g1 = r1.x;
         out.g2 = r1.y;
         if constexpr (IB == IB_SUBCRITICAL) {
-            out.k = kappa_eval(fx, fy, fz);   // cl_lo is in tau_scale
+            out.k = kappa_eval(fx, fy, fz);   // cl_lo / ope2^2 is in tau_scale
         } else if constexpr (IB == IB_GENERAL) {
             out.k = kappa_eval(fx, fy, fz);
         } else {
@@ -415,20 +411,20 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
             poly_coeffs<R>(cc.t[2], v0.z, v1.z, v2.z, v3.z, v4.z, v5.z, v6.z, v7.z);
             poly_coeffs<R>(cc.t[3], v0.w, v1.w, v2.w, v3.w, v4.w, v5.w, v6.w, v7.w);
             if constexpr (IB == IB_SUBCRITICAL) {
-                poly_coeffs<R>(cc.t[4 % (IB ? 5 : 4)], v0.x * v0.x, v1.x * v1.x, v2.x * v2.x, v3.x * v3.x,
-                               v4.x * v4.x, v5.x * v5.x, v6.x * v6.x, v7.x * v7.x);
+                poly_coeffs<R>(cc.t[4 % (IB ? 5 : 4)], corner_x2(v0.x), corner_x2(v1.x), corner_x2(v2.x),
+                               corner_x2(v3.x), corner_x2(v4.x), corner_x2(v5.x), corner_x2(v6.x), corner_x2(v7.x));
             } else if constexpr (IB == IB_GENERAL) {
                 poly_coeffs<R>(cc.t[4 % (IB ? 5 : 4)], corner_kappa<P>(a, v0.x), corner_kappa<P>(a, v1.x),
                                corner_kappa<P>(a, v2.x), corner_kappa<P>(a, v3.x), corner_kappa<P>(a, v4.x),
                                corner_kappa<P>(a, v5.x), corner_kappa<P>(a, v6.x), corner_kappa<P>(a, v7.x));
             }
         }
-        out.q = poly_eval<R>(cc.t[0], fx, fy, fz);
+        out.n1 = poly_eval<R>(cc.t[0], fx, fy, fz);
         out.g0 = poly_eval<R>(cc.t[1], fx, fy, fz);
         out.g1 = poly_eval<R>(cc.t[2], fx, fy, fz);
         out.g2 = poly_eval<R>(cc.t[3], fx, fy, fz);
         if constexpr (IB == IB_SUBCRITICAL) {
-            out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz);   // cl_lo is in tau_scale
+            out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz);   // cl_lo / ope2^2 is in tau_scale
         } else if constexpr (IB == IB_GENERAL) {
             out.k = poly_eval<R>(cc.t[4 % (IB ? 5 : 4)], fx, fy, fz);
         } else {
@@ -471,15 +467,15 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
             g1 += c[i].z * w[i];
             g2 += c[i].w * w[i];
         }
-        out.q = q;
+        out.n1 = q;
         out.g0 = g0;
         out.g1 = g1;
         out.g2 = g2;
         if constexpr (IB == IB_SUBCRITICAL) {
             R k = R(0);
     #pragma unroll
-            for (int i = 0; i < 8; ++i) k += w[i] * (c[i].x * c[i].x);
-            out.k = k;   // cl_lo is in tau_scale
+            for (int i = 0; i < 8; ++i) k += w[i] * corner_x2(c[i].x);
+            out.k = k;   // cl_lo / ope2^2 is in tau_scale
         } else if constexpr (IB == IB_GENERAL) {
             R k = R(0);
     #pragma unroll
@@ -504,15 +500,14 @@ __device__ __forceinline__ void sample_c(const TraceArgs& a, const typename P::R
 // order in the step (their middle stage point is second order), an error
 // many orders below the FP32 rounding here. Stage sums are accumulated as the
 // stages are produced to keep few values live.
-// The phase integrand is n - 1 with n = sqrt(1 - (omega_pe/omega)^2) from the
-// interpolated density (src/legacy/full_solver.py:271-274, :341-347).
-template <class P, int IB, bool SMALLX, int MODE, class Cache>
+// The phase integrand n - 1 is interpolated from the trace layout's channel 0
+// (the legacy solver's interpolated n, src/legacy/full_solver.py:289, :342-345).
+template <class P, int IB, int MODE, class Cache>
 __device__ __forceinline__ void rkn_step(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
     using R = typename P::R;
     const R hphi = R(0.5) * phi, phi6 = phi * R(1.0 / 6.0), phi2_6 = phi * phi6;
     const R phi2_8 = R(0.125) * phi * phi, phi2_2 = R(0.5) * phi * phi;
     const R S0 = arg_S<R>(a, 0), S1 = arg_S<R>(a, 1), S2 = arg_S<R>(a, 2);
-    const R ope2 = arg_ope2<R>(a);
     R ph[3], pl[3], we[3], sA[3], sW[3], st[3];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
@@ -521,17 +516,9 @@ __device__ __forceinline__ void rkn_step(const TraceArgs& a, Ray<P>& r, Cache& c
         we[x] = r.w[x].val();
     }
     Sample<P> s;
-    // FP32 with the series form of n - 1 evaluates it for stages 1 and 2 as a pair
-    constexpr bool kPairPhase = SMALLX && sizeof(R) == 4;
     // stage 1 at p
     sample_c<P, IB, MODE>(a, ph, pl, s, cc);
-    R g, q1 = R(0);
-    if constexpr (kPairPhase) {
-        q1 = s.q;
-        g = R(0);
-    } else {
-        g = nm1<P, SMALLX>(ope2 * s.q);
-    }
+    R g = s.n1;
     R kq = s.k;
     {
         const R A[3] = {S0 * s.g0, S1 * s.g1, S2 * s.g2};
@@ -553,17 +540,12 @@ __device__ __forceinline__ void rkn_step(const TraceArgs& a, Ray<P>& r, Cache& c
             st[x] = pl[x] + (phi * we[x] + phi2_2 * A[x]);      // p + phi*w + phi^2 A2/2
         }
     }
-    if constexpr (kPairPhase) {
-        const float2 n12 = nm1_series2(__fmul2_rn(make_float2(ope2, ope2), make_float2(q1, s.q)));
-        g = n12.x + R(4) * n12.y;
-    } else {
-        g += R(4) * nm1<P, SMALLX>(ope2 * s.q);
-    }
+    g += R(4) * s.n1;
     kq += R(4) * s.k;
     // stage 3
     sample_c<P, IB, MODE>(a, ph, st, s, cc);
     sW[0] += S0 * s.g0; sW[1] += S1 * s.g1; sW[2] += S2 * s.g2;
-    g += nm1<P, SMALLX>(ope2 * s.q);
+    g += s.n1;
     kq += s.k;
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
@@ -604,7 +586,7 @@ __device__ __forceinline__ void sample_f2(const TraceArgs& a, float hx, float lx
         const bool in = (px >= 0.0f) & (px <= g.limf[0]) & (pyz.x >= 0.0f) & (pyz.x <= g.limf[1]) &
                         (pyz.y >= 0.0f) & (pyz.y <= g.limf[2]);
         if (!in) {
-            out.q = out.g0 = out.g1 = out.g2 = out.k = 0.0f;
+            out.n1 = out.g0 = out.g1 = out.g2 = out.k = 0.0f;
             return;
         }
         ix = min((int)px, g.n[0] - 2);
@@ -622,12 +604,12 @@ __device__ __forceinline__ void sample_f2(const TraceArgs& a, float hx, float lx
     const float2 fx2 = bc2(fx), fy2 = bc2(fyz.x), fz2 = bc2(fyz.y);
     const float2 r0 = poly_eval2(cc.t[0], fx2, fy2, fz2);
     const float2 r1 = poly_eval2(cc.t[1], fx2, fy2, fz2);
-    out.q = r0.x;
+    out.n1 = r0.x;
     out.g0 = r0.y;
     out.g1 = r1.x;
     out.g2 = r1.y;
     if constexpr (IB == IB_SUBCRITICAL) {
-        out.k = kappa_eval(fx, fyz.x, fyz.y);   // cl_lo is in tau_scale
+        out.k = kappa_eval(fx, fyz.x, fyz.y);   // cl_lo / ope2^2 is in tau_scale
     } else if constexpr (IB == IB_GENERAL) {
         out.k = kappa_eval(fx, fyz.x, fyz.y);
     } else {
@@ -646,7 +628,7 @@ __device__ __forceinline__ void kahan2(float2& s, float2& c, float2 x) {
 // UNIT: phi is 1 (every step but a cut one); the multiplications by phi are
 // left out, which gives bitwise the results of the general form at phi = 1
 // (fma(1, a, b) rounds as a + b).
-template <int IB, bool SMALLX, int MODE, bool UNIT, int NK>
+template <int IB, int MODE, bool UNIT, int NK>
 __device__ __forceinline__ void rkn_step_f2(const TraceArgs& a, Ray<PolF32>& r, CellPolyF2<NK>& cc, float phi) {
     if constexpr (UNIT) phi = 1.0f;
     auto mphi = [&](float x) { return UNIT ? x : __fmul_rn(phi, x); };
@@ -655,19 +637,16 @@ __device__ __forceinline__ void rkn_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
     const float phi2_8 = 0.125f * phi * phi, phi2_2 = 0.5f * phi * phi;
     const float S0 = a.Sf[0];
     const float2 S12 = make_float2(a.Sf[1], a.Sf[2]);
-    const float ope2 = a.ope2f;
     const float2 hphi2 = bc2(hphi), phi22 = bc2(phi), phi2_82 = bc2(phi2_8), phi2_22 = bc2(phi2_2);
     // Every rounding is explicit (intrinsics), so that each kernel that
     // inlines this step (the tracer's and the server's) rounds alike.
     const float phx = r.p[0].s, plx = r.p[0].c, wex = r.w[0].s + r.w[0].c;
     const float2 phyz = make_float2(r.p[1].s, r.p[2].s), plyz = make_float2(r.p[1].c, r.p[2].c);
     const float2 weyz = __fadd2_rn(make_float2(r.w[1].s, r.w[2].s), make_float2(r.w[1].c, r.w[2].c));
-    constexpr bool kPairPhase = SMALLX;
     Sample<PolF32> s;
     // stage 1 at p
     sample_f2<IB, MODE>(a, phx, plx, phyz, plyz, s, cc);
-    float g = 0.0f, q1 = 0.0f;
-    if constexpr (kPairPhase) q1 = s.q; else g = nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q));
+    float g = s.n1;
     float kq = s.k;
     float sAx = __fmul_rn(S0, s.g0);
     float2 sAyz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
@@ -688,20 +667,12 @@ __device__ __forceinline__ void rkn_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
         stx = __fadd_rn(plx, __fmaf_rn(phi2_2, Ax, mphi(wex)));
         styz = __fadd2_rn(plyz, __ffma2_rn(phi2_22, Ayz, mphi2(weyz)));
     }
-    if constexpr (kPairPhase) {
-        const float2 n12 = nm1_series2(__fmul2_rn(bc2(ope2), make_float2(q1, s.q)));
-        g = __fmaf_rn(4.0f, n12.y, n12.x);
-    } else {
-        g = __fmaf_rn(4.0f, nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q)), g);
-    }
+    g = __fmaf_rn(4.0f, s.n1, g);
     kq = __fmaf_rn(4.0f, s.k, kq);
     sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
     sWx = __fmaf_rn(S0, s.g0, sWx);
     sWyz = __ffma2_rn(S12, make_float2(s.g1, s.g2), sWyz);
-    if constexpr (kPairPhase)
-        g = __fadd_rn(g, nm1_series1(__fmul_rn(ope2, s.q)));
-    else
-        g = __fadd_rn(g, nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q)));
+    g = __fadd_rn(g, s.n1);
     kq = __fadd_rn(kq, s.k);
     // x: the scalar update
     if constexpr (UNIT)
@@ -735,13 +706,12 @@ __device__ __forceinline__ void rkn_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
 // The stage points lie within phi^2 |A|/4 and phi^2 |A|/2 of the segment
 // from p to p + phi*w, as the RKN step's do, so the interior-sampling bound
 // kInteriorAccel and the interior-run envelope hold for both methods.
-template <class P, int IB, bool SMALLX, int MODE, class Cache>
+template <class P, int IB, int MODE, class Cache>
 __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
     using R = typename P::R;
     const R two = R(2);
     const R hphi = R(0.5) * phi, phi6 = phi * R(1.0 / 6.0), phi2_6 = phi * phi6;
     const R S0 = arg_S<R>(a, 0), S1 = arg_S<R>(a, 1), S2 = arg_S<R>(a, 2);
-    const R ope2 = arg_ope2<R>(a);
     R ph[3], pl[3], we[3], sA[3], sW[3], w3[3], st[3];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
@@ -750,18 +720,9 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
         we[x] = r.w[x].val();
     }
     Sample<P> s;
-    // FP32 with the series form of n - 1 evaluates it for stages (1, 2) and
-    // (3, 4) as pairs
-    constexpr bool kPairPhase = SMALLX && sizeof(R) == 4;
     // stage 1 at p
     sample_c<P, IB, MODE>(a, ph, pl, s, cc);
-    R g, q1 = R(0), q3 = R(0);
-    if constexpr (kPairPhase) {
-        q1 = s.q;
-        g = R(0);
-    } else {
-        g = nm1<P, SMALLX>(ope2 * s.q);
-    }
+    R g = s.n1;
     R kq = s.k;
     sA[0] = S0 * s.g0; sA[1] = S1 * s.g1; sA[2] = S2 * s.g2;
     // stage 2 at p + phi*w/2
@@ -782,12 +743,7 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
             sW[x] += two * A[x];
         }
     }
-    if constexpr (kPairPhase) {
-        const float2 n12 = nm1_series2(__fmul2_rn(make_float2(ope2, ope2), make_float2(q1, s.q)));
-        g = n12.x + two * n12.y;
-    } else {
-        g += two * nm1<P, SMALLX>(ope2 * s.q);
-    }
+    g += two * s.n1;
     kq += two * s.k;
     // stage 3 at p + phi*w2/2
     sample_c<P, IB, MODE>(a, ph, st, s, cc);
@@ -800,21 +756,12 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
             st[x] = pl[x] + phi * w3[x];
         }
     }
-    if constexpr (kPairPhase) {
-        q3 = s.q;
-    } else {
-        g += two * nm1<P, SMALLX>(ope2 * s.q);
-    }
+    g += two * s.n1;
     kq += two * s.k;
     // stage 4 at p + phi*w3
     sample_c<P, IB, MODE>(a, ph, st, s, cc);
     sW[0] += S0 * s.g0; sW[1] += S1 * s.g1; sW[2] += S2 * s.g2;
-    if constexpr (kPairPhase) {
-        const float2 n34 = nm1_series2(__fmul2_rn(make_float2(ope2, ope2), make_float2(q3, s.q)));
-        g += two * n34.x + n34.y;
-    } else {
-        g += nm1<P, SMALLX>(ope2 * s.q);
-    }
+    g += s.n1;
     kq += s.k;
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
@@ -827,24 +774,21 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
 }
 
 // The RK4 step in the paired FP32 form (y and z components as register
-// pairs), rounded exactly as the scalar form rounds each component.
-template <int IB, bool SMALLX, int MODE, bool UNIT, int NK>
+// pairs), every rounding explicit.
+template <int IB, int MODE, bool UNIT, int NK>
 __device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, CellPolyF2<NK>& cc, float phi) {
     if constexpr (UNIT) phi = 1.0f;
     const float hphi = 0.5f * phi, phi6 = phi * (1.0f / 6.0f), phi2_6 = phi * phi6;
     const float S0 = a.Sf[0];
     const float2 S12 = make_float2(a.Sf[1], a.Sf[2]);
-    const float ope2 = a.ope2f;
     const float2 hphi2 = bc2(hphi), two2 = bc2(2.0f);
     const float phx = r.p[0].s, plx = r.p[0].c, wex = __fadd_rn(r.w[0].s, r.w[0].c);
     const float2 phyz = make_float2(r.p[1].s, r.p[2].s), plyz = make_float2(r.p[1].c, r.p[2].c);
     const float2 weyz = __fadd2_rn(make_float2(r.w[1].s, r.w[2].s), make_float2(r.w[1].c, r.w[2].c));
-    constexpr bool kPairPhase = SMALLX;
     Sample<PolF32> s;
     // stage 1 at p
     sample_f2<IB, MODE>(a, phx, plx, phyz, plyz, s, cc);
-    float g = 0.0f, q1 = 0.0f, q3 = 0.0f;
-    if constexpr (kPairPhase) q1 = s.q; else g = nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q));
+    float g = s.n1;
     float kq = s.k;
     float sAx = __fmul_rn(S0, s.g0);
     float2 sAyz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
@@ -868,12 +812,7 @@ __device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
         sWx = __fmaf_rn(2.0f, Ax, sWx);
         sWyz = __ffma2_rn(two2, Ayz, sWyz);
     }
-    if constexpr (kPairPhase) {
-        const float2 n12 = nm1_series2(__fmul2_rn(bc2(ope2), make_float2(q1, s.q)));
-        g = __fmaf_rn(2.0f, n12.y, n12.x);
-    } else {
-        g = __fmaf_rn(2.0f, nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q)), g);
-    }
+    g = __fmaf_rn(2.0f, s.n1, g);
     kq = __fmaf_rn(2.0f, s.k, kq);
     // stage 3 at p + phi*w2/2
     sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
@@ -887,18 +826,13 @@ __device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
         stx = __fmaf_rn(phi, w3x, plx);
         styz = __ffma2_rn(bc2(phi), w3yz, plyz);
     }
-    if constexpr (kPairPhase) q3 = s.q; else g = __fmaf_rn(2.0f, nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q)), g);
+    g = __fmaf_rn(2.0f, s.n1, g);
     kq = __fmaf_rn(2.0f, s.k, kq);
     // stage 4 at p + phi*w3
     sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
     sWx = __fmaf_rn(S0, s.g0, sWx);
     sWyz = __ffma2_rn(S12, make_float2(s.g1, s.g2), sWyz);
-    if constexpr (kPairPhase) {
-        const float2 n34 = nm1_series2(__fmul2_rn(bc2(ope2), make_float2(q3, s.q)));
-        g = __fadd_rn(g, __fmaf_rn(2.0f, n34.x, n34.y));
-    } else {
-        g = __fadd_rn(g, nm1<PolF32, SMALLX>(__fmul_rn(ope2, s.q)));
-    }
+    g = __fadd_rn(g, s.n1);
     kq = __fadd_rn(kq, s.k);
     // x: the scalar update
     r.p[0].add(__fmaf_rn(phi, r.w[0].hi(), __fmaf_rn(phi, r.w[0].lo(), __fmul_rn(phi2_6, sAx))));
@@ -921,18 +855,18 @@ __device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
 
 // One step: the paired FP32 form with the paired cell cache, the generic form
 // otherwise; RKN unless INTEG selects RK4.
-template <class P, int IB, bool SMALLX, int MODE, bool UNIT = false, int INTEG = INTEG_RKN, class Cache>
+template <class P, int IB, int MODE, bool UNIT = false, int INTEG = INTEG_RKN, class Cache>
 __device__ __forceinline__ void step_any(const TraceArgs& a, Ray<P>& r, Cache& cc, typename P::R phi) {
     if constexpr (INTEG == INTEG_RK4) {
         if constexpr (IsPairedCache<Cache>::value && SLOTH_PAIRED_STEP) {
-            rk4_step_f2<IB, SMALLX, MODE, UNIT>(a, r, cc, phi);
+            rk4_step_f2<IB, MODE, UNIT>(a, r, cc, phi);
         } else {
-            rk4_step<P, IB, SMALLX, MODE>(a, r, cc, phi);
+            rk4_step<P, IB, MODE>(a, r, cc, phi);
         }
     } else if constexpr (IsPairedCache<Cache>::value && SLOTH_PAIRED_STEP) {
-        rkn_step_f2<IB, SMALLX, MODE, UNIT>(a, r, cc, phi);
+        rkn_step_f2<IB, MODE, UNIT>(a, r, cc, phi);
     } else {
-        rkn_step<P, IB, SMALLX, MODE>(a, r, cc, phi);
+        rkn_step<P, IB, MODE>(a, r, cc, phi);
     }
 }
 
@@ -1192,7 +1126,7 @@ __device__ __forceinline__ void tile_sort(unsigned* key, unsigned* id, int size)
 // acceleration bound skip it and sample without the grid test (bound at most
 // kInteriorAccel); 2 they skip the face test but sample with the grid test
 // (any finite bound). Every mode takes the same steps.
-template <class P, int IB, bool SMALLX, int FAST, int INTEG = INTEG_RKN, class Cache>
+template <class P, int IB, int FAST, int INTEG = INTEG_RKN, class Cache>
 __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, int cnt, unsigned* s_key,
                                            unsigned* s_id, int* s_head, Cache& cc,
                                            unsigned long long& my_steps) {
@@ -1257,16 +1191,16 @@ __device__ __forceinline__ void trace_tile(const TraceArgs& a, long long start, 
             if (FAST && kind == 0) {
 #pragma unroll 1
                 for (int e = 0;; ++e) {
-                    step_any<P, IB, SMALLX, FAST == 1 ? SAMPLE_INTERIOR : SAMPLE_PLAIN, true, INTEG>(
+                    step_any<P, IB, FAST == 1 ? SAMPLE_INTERIOR : SAMPLE_PLAIN, true, INTEG>(
                         a, r, cc, typename P::R(1));
                     if (e == extra) break;
                     ++r.step;
                 }
                 r.run -= extra;
             } else if (kind == 0 || kind == 3) {
-                step_any<P, IB, SMALLX, SAMPLE_PLAIN, true, INTEG>(a, r, cc, typename P::R(1));
+                step_any<P, IB, SAMPLE_PLAIN, true, INTEG>(a, r, cc, typename P::R(1));
             } else {
-                step_any<P, IB, SMALLX, SAMPLE_CLAMP, false, INTEG>(a, r, cc, phi);
+                step_any<P, IB, SAMPLE_CLAMP, false, INTEG>(a, r, cc, phi);
                 if (kind == 2) {
                     r.exited = true;
                     r.lag = 1.0 - (double)phi;
@@ -1484,11 +1418,11 @@ inline int launch_prepass(const SlothGridDesc* g, int axis, const R* rays, long 
     return cuda_status(cudaGetLastError());
 }
 
-// Tracer mode of a trace: inverse-bremsstrahlung path and phase form.
-inline void trace_mode(const SlothTraceParams* p, int* ib, bool* smallx) {
+// Inverse-bremsstrahlung path of a trace: off, sub-critical (the grid's
+// density stays below nc, so the Coulomb log is a constant), or general.
+inline int trace_mode(const SlothTraceParams* p) {
     const double xmax = p->q_max > 0.0 ? p->q_max * p->ope_ratio2 : 1e300;
-    *smallx = xmax <= kSmallX;
-    *ib = !p->inv_brems ? IB_OFF : (xmax <= 1.0 ? IB_SUBCRITICAL : IB_GENERAL);
+    return !p->inv_brems ? IB_OFF : (xmax <= 1.0 ? IB_SUBCRITICAL : IB_GENERAL);
 }
 
 // Largest |acceleration| (cells per step^2) the grid's density range allows:
@@ -1532,16 +1466,13 @@ inline void fill_trace_args(TraceArgs& ta, const SlothGridDesc* g, const void* g
     ta.cl_lo = p->coulomb_log_w > 2.0 ? p->coulomb_log_w : 2.0;
     ta.ope2 = p->ope_ratio2;
     ta.ope2f = (float)ta.ope2;
+    ta.inv_ope2 = 1.0 / p->ope_ratio2;
+    ta.inv_ope2f = (float)ta.inv_ope2;
     ta.cl_lof = (float)ta.cl_lo;
-    {
-        // Below the critical density the Coulomb log is the constant cl_lo, so
-        // the sub-critical samples leave it out of kappa and the optical
-        // depth's scale takes it once.
-        int ib;
-        bool smallx;
-        trace_mode(p, &ib, &smallx);
-        if (ib == IB_SUBCRITICAL) ta.tau_scale *= ta.cl_lo;
-    }
+    // Below the critical density the Coulomb log is the constant cl_lo and the
+    // corners carry x^2 = (ope2 q)^2, so the optical depth's scale takes
+    // cl_lo / ope2^2 once.
+    if (trace_mode(p) == IB_SUBCRITICAL) ta.tau_scale *= ta.cl_lo * ta.inv_ope2 * ta.inv_ope2;
     ta.cl_wf = (float)ta.cl_w;
     {
         const double B = interior_accel_bound(g, p);
@@ -1580,6 +1511,7 @@ inline int check_trace_params(const SlothGridDesc* g, const SlothTraceParams* p,
     if (last > 2000000000LL) return SLOTH_ERR_TOO_LARGE;
     if (p->inv_brems && !(p->kappa_q2 >= 0.0)) return SLOTH_ERR_INVALID_ARGUMENT;
     if (p->project_to_plane && !std::isfinite(p->plane)) return SLOTH_ERR_INVALID_ARGUMENT;
+    if (!(p->ope_ratio2 > 0.0) || !std::isfinite(p->ope_ratio2)) return SLOTH_ERR_INVALID_ARGUMENT;
     if (!std::isfinite(p->q_max)) return SLOTH_ERR_INVALID_ARGUMENT;
     if (p->integrator != SLOTH_INTEGRATOR_RKN && p->integrator != SLOTH_INTEGRATOR_RK4)
         return SLOTH_ERR_INVALID_ARGUMENT;

@@ -53,7 +53,9 @@ def uniform_axis(coords) -> tuple[float, float, int]:
 
 @dataclass
 class DeviceGrid:
-    """A packed (q, dq/du, dq/dv, dq/dw) grid resident in HBM."""
+    """A packed (c0, dq/du, dq/dv, dq/dw) grid resident in HBM: c0 = n - 1 in
+    the trace layout (what the tracers read), c0 = q in the value layout (the
+    K0 sampler's)."""
     data: torch.Tensor
     desc: capi.SlothGridDesc
     precision: str
@@ -64,6 +66,7 @@ class DeviceGrid:
     q_max: float = 0.0         # max of the q channel (ne/nc) over the grid; 0 = unknown
     q_min: float = float("inf")  # a lower bound of min(q, 0) over the grid; inf = unknown
     ne_max: float = float("nan")  # largest ne (m^-3) packed, from the device reduction
+    layout: str = "trace"
 
     @property
     def nc(self) -> float:
@@ -79,13 +82,18 @@ class DeviceGrid:
 
 
 def pack_grid(ne, origin, spacing, omega, *, precision="f32", device=None, stream=None,
-              out: Optional[torch.Tensor] = None, ne_scale: Optional[float] = None) -> DeviceGrid:
+              out: Optional[torch.Tensor] = None, ne_scale: Optional[float] = None,
+              layout: str = "trace") -> DeviceGrid:
     """K1: pack ne (m^-3, (nx, ny, nz) array or tensor) into a device grid.
 
     ``ne`` may be a numpy array, a CPU tensor (pinned for a fast copy) or a
-    CUDA tensor; float32 and float64 are read as they are. The q channel is
-    ne * ne_scale with ne_scale = 1/nc(omega) unless given.
+    CUDA tensor; float32 and float64 are read as they are. q = ne * ne_scale
+    with ne_scale = 1/nc(omega) unless given. ``layout`` 'trace' (the
+    tracers' grid) stores n - 1 of the plasma refractive index in channel 0,
+    'values' stores q there (for the K0 sampler).
     """
+    if layout not in ("trace", "values"):
+        raise ValueError("layout must be 'trace' or 'values'")
     dev = require_device(device)
     if isinstance(ne, np.ndarray):
         ne = torch.from_numpy(np.ascontiguousarray(ne))
@@ -104,10 +112,16 @@ def pack_grid(ne, origin, spacing, omega, *, precision="f32", device=None, strea
         raise ValueError(f"invalid grid {n}")
     if out is None:
         out = torch.empty(nbytes // rb, dtype=torch.float32 if rb == 4 else torch.float64, device=dev)
-    fn = capi.load().sloth_grid_pack_f32 if precision == "f32" else capi.load().sloth_grid_pack_f64
     scale = 1.0 / physics.critical_density(omega) if ne_scale is None else float(ne_scale)
-    capi.check(fn(desc, capi.ptr(ne), int(ne.dtype == torch.float64), scale, capi.ptr(out), _stream_ptr(stream)),
-               "sloth_grid_pack")
+    lib = capi.load()
+    if layout == "trace":
+        fn = lib.sloth_grid_pack_trace_f32 if precision == "f32" else lib.sloth_grid_pack_trace_f64
+        capi.check(fn(desc, capi.ptr(ne), int(ne.dtype == torch.float64), scale, physics.ope_ratio2(omega),
+                      capi.ptr(out), _stream_ptr(stream)), "sloth_grid_pack_trace")
+    else:
+        fn = lib.sloth_grid_pack_f32 if precision == "f32" else lib.sloth_grid_pack_f64
+        capi.check(fn(desc, capi.ptr(ne), int(ne.dtype == torch.float64), scale, capi.ptr(out),
+                      _stream_ptr(stream)), "sloth_grid_pack")
     if ne.numel():
         lo, hi = torch.aminmax(ne)
         ne_max = float(hi)
@@ -115,11 +129,13 @@ def pack_grid(ne, origin, spacing, omega, *, precision="f32", device=None, strea
     else:
         ne_max, q_max, q_min = 0.0, 0.0, 0.0
     return DeviceGrid(out, desc, precision, float(omega), n, tuple(map(float, origin)), tuple(map(float, spacing)),
-                      q_max=max(q_max, 0.0) * (1.0 + 1e-6), q_min=min(q_min, 0.0) * (1.0 + 1e-6), ne_max=ne_max)
+                      q_max=max(q_max, 0.0) * (1.0 + 1e-6), q_min=min(q_min, 0.0) * (1.0 + 1e-6), ne_max=ne_max,
+                      layout=layout)
 
 
 def sample(grid: DeviceGrid, points, *, stream=None) -> torch.Tensor:
-    """K0: (4, N) interpolated (q, dq/du, dq/dv, dq/dw) at points (3, N) in metres."""
+    """K0: (4, N) interpolated (c0, dq/du, dq/dv, dq/dw) at points (3, N) in
+    metres (c0 = q in the value layout)."""
     pts = torch.as_tensor(points, dtype=torch.float64)
     pts = pts.to(grid.data.device).contiguous()
     n = pts.shape[1]
@@ -204,6 +220,8 @@ def trace(grid: DeviceGrid, rays: torch.Tensor, sched: Schedule, *, axis=2, proj
     optional pair of recorded torch.cuda.Event(enable_timing=True) that the
     library re-records around the tracer kernel alone.
     """
+    if grid.layout != "trace":
+        raise ValueError("the tracers read grids packed with layout='trace'")
     dtype = torch.float32 if grid.precision == "f32" else torch.float64
     if rays.dtype != dtype or rays.device != grid.data.device or not rays.is_contiguous():
         rays = rays.to(device=grid.data.device, dtype=dtype).contiguous()

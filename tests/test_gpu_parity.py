@@ -19,22 +19,29 @@ from conftest import golden
 from helpers import C, case, direction_error, position_error, run_kernel, run_oracle
 from oracle import ref_restated as rr
 from sloth_b200 import _capi, runtime, workloads
+from sloth_b200.core import physics
 
 pytestmark = pytest.mark.gpu
 
 L = 5e-3
 
 
+@pytest.mark.parametrize("layout", ["trace", "values"])
 @pytest.mark.parametrize("ne_dtype", [np.float32, np.float64])
-def test_pack_matches_oracle_bitwise(ne_dtype):
+def test_pack_matches_oracle_bitwise(ne_dtype, layout):
+    """Both layouts of K1, bitwise the oracle's FP64 formula (the trace
+    layout's n - 1 includes densities above the critical one, where it is -x)."""
     rng = np.random.RandomState(5)
     ne = rng.uniform(1e24, 3e25, size=(9, 10, 11)).astype(ne_dtype)
     omega = 2 * np.pi * C / 532e-9
-    scale = 1.0 / rr.critical_density(omega)
-    ref = rr.pack_grid(ne.astype(np.float64), scale)
-    g64 = runtime.pack_grid(torch.from_numpy(ne), (0, 0, 0), (1e-5,) * 3, omega, precision="f64")
+    nc = rr.critical_density(omega)
+    ne[0, 0, :3] = np.array([0.5, 0.999, 2.0]) * nc
+    scale = 1.0 / nc
+    ope2 = physics.ope_ratio2(omega) if layout == "trace" else None
+    ref = rr.pack_grid(ne.astype(np.float64), scale, ope2)
+    g64 = runtime.pack_grid(torch.from_numpy(ne), (0, 0, 0), (1e-5,) * 3, omega, precision="f64", layout=layout)
     np.testing.assert_array_equal(g64.data.view(9, 10, 11, 4).cpu().numpy(), ref)
-    g32 = runtime.pack_grid(torch.from_numpy(ne), (0, 0, 0), (1e-5,) * 3, omega, precision="f32")
+    g32 = runtime.pack_grid(torch.from_numpy(ne), (0, 0, 0), (1e-5,) * 3, omega, precision="f32", layout=layout)
     np.testing.assert_array_equal(g32.data.view(9, 10, 11, 4).cpu().numpy(), ref.astype(np.float32))
 
 
@@ -44,7 +51,8 @@ def test_sample_matches_reference_interpolator(precision, rtol):
     x, y, z = g["x"], g["y"], g["z"]
     origin = (x[0], y[0], z[0])
     spacing = tuple((a[-1] - a[0]) / (a.size - 1) for a in (x, y, z))
-    grid = runtime.pack_grid(torch.from_numpy(g["values"]), origin, spacing, 1.0, precision=precision, ne_scale=1.0)
+    grid = runtime.pack_grid(torch.from_numpy(g["values"]), origin, spacing, 1.0, precision=precision, ne_scale=1.0,
+                             layout="values")
     got = runtime.sample(grid, g["points"].T)[0].cpu().numpy().astype(np.float64)
     scale = np.abs(g["values"]).max()
     np.testing.assert_allclose(got, g["result"], rtol=0, atol=rtol * scale)

@@ -251,10 +251,24 @@ def test_reference_phase_integrand_golden(name):
 
 
 @pytest.mark.parametrize("name", PHASE_CASES)
-def test_kernel_phase_integrand_equals_reference_at_nodes(name):
-    """The tracers take n from the interpolated density, n(interp(ne)); the
-    legacy solver interpolates n. The two agree at grid nodes, and between
-    nodes differ by the curvature of n(ne) over one cell."""
+def test_trace_layout_phase_channel_golden(name):
+    """The tracers interpolate channel 0 of the trace layout, n - 1 at the grid
+    points (rr.pack_grid with ope_ratio2, the K1 formula): times omega it is
+    the legacy solver's ScalarDomain.phase at every golden point."""
+    g = golden("phase")
+    ne, pts, ref = g[f"{name}_ne"], g[f"{name}_points"], g[f"{name}_phase"]
+    ax = [g[f"{name}_{a}"] for a in "xyz"]
+    omega = float(g[f"{name}_omega"])
+    packed = rr.pack_grid(ne, 1.0 / rr.critical_density(omega), rr.ope_ratio2(omega))
+    got = omega * rr.regular_grid_interpolator(tuple(ax), packed[..., 0], pts.T)
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("name", PHASE_CASES)
+def test_density_phase_integrand_equals_reference_at_nodes(name):
+    """The other semantics, n from the interpolated density (the oracle's
+    phase_mode 'density'), agrees with the legacy solver at grid nodes and
+    differs between them by the curvature of n(ne) over one cell."""
     g = golden("phase")
     ne, pts, ref = g[f"{name}_ne"], g[f"{name}_points"], g[f"{name}_phase"]
     ax = [g[f"{name}_{a}"] for a in "xyz"]
