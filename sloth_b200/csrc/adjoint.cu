@@ -43,13 +43,8 @@
 namespace sloth {
 
 constexpr int kAdjThreads = 256;
-// The backward keeps the inputs of a checkpoint segment's steps in shared
-// memory: (p_hi, p_lo, w) per step, 9 floats in FP32 (6 doubles in FP64,
-// whose positions carry no compensation), [step][word][thread] so that a
-// warp's accesses are consecutive. 128 threads per CTA: a 20-step segment
-// takes 92 KB in FP32, so two CTAs share an SM.
-constexpr int kAdjBwdThreads = 128;
-template <class P> constexpr int adj_state_words() { return sizeof(typename P::R) == 4 ? 9 : 6; }
+// The FP32 backward fits in 128 registers (two 256-thread CTAs per SM) with a
+// few bytes of spill; the FP64 one would spill kilobytes, so it keeps one.
 template <class P> constexpr int adj_bwd_min_blocks() { return sizeof(typename P::R) == 4 ? 2 : 1; }
 // The FP32 forward fits three 256-thread CTAs per SM (80 registers) without spilling.
 template <class P> constexpr int adj_fwd_min_blocks() { return sizeof(typename P::R) == 4 ? 3 : 1; }
@@ -424,22 +419,22 @@ __device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const typename
         for (int c = 0; c < 8; ++c) acc.v[k][c] += gb[k] * w[c];
 }
 
-// Reverse of model_step from the step's input (p = ph + pl, w = we): (lp,
-// lw) = adjoint of the output (p', w') on entry, of the input (p, w) on
-// return. The first two stage accelerations, which place stages 2 and 3,
-// are evaluated again here as model_step evaluates them, so that the
-// segment buffer holds only the step inputs.
+// Reverse of model_step from the step's input state r: (lp, lw) = adjoint of
+// the output (p', w') on entry, of the input (p, w) on return.
 template <class P, class Cell, class Acc>
-__device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const typename P::R (&ph)[3],
-                                                   const typename P::R (&pl)[3], const typename P::R (&we)[3],
+__device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const MState<P>& r,
+                                                   const typename P::R (&A1)[3], const typename P::R (&A2)[3],
                                                    typename P::R (&lp)[3], typename P::R (&lw)[3], Cell& cc,
                                                    Acc& acc) {
     using R = typename P::R;
-    R st[3], A1[3], A2[3];
-    accel<P, false>(a, ph, pl, A1, cc);
+    R ph[3], pl[3], we[3], st[3];
 #pragma unroll
-    for (int x = 0; x < 3; ++x) st[x] = pl[x] + (R(0.5) * we[x] + R(0.125) * A1[x]);
-    accel<P, false>(a, ph, st, A2, cc);
+    for (int x = 0; x < 3; ++x) {
+        ph[x] = r.p[x].hi();
+        pl[x] = r.p[x].lo();
+        we[x] = r.w[x].val();
+    }
+    // A1, A2 (which place stages 2 and 3) come from the segment's recompute.
     // Direct terms of p' = p + w + (A1 + 2 A2)/6, w' = w + (A1 + 4 A2 + A3)/6:
     R a1[3], a2[3], a3[3], pb[3], wb[3], q[3];
 #pragma unroll
@@ -729,37 +724,9 @@ __global__ void __launch_bounds__(kAdjThreads, adj_fwd_min_blocks<P>()) image_fo
     block_add((unsigned long long)t, &s_steps, a.total_steps);
 }
 
-// Input of step j of the current segment into / out of the shared buffer.
 template <class P>
-__device__ __forceinline__ void put_step(typename P::R* buf, int j, const MState<P>& r) {
-    constexpr int NW = adj_state_words<P>();
-    typename P::R* b = buf + (size_t)j * NW * kAdjBwdThreads;
-#pragma unroll
-    for (int x = 0; x < 3; ++x) {
-        b[x * kAdjBwdThreads] = r.p[x].hi();
-        b[(3 + x) * kAdjBwdThreads] = r.w[x].val();
-        if constexpr (NW == 9) b[(6 + x) * kAdjBwdThreads] = r.p[x].lo();
-    }
-}
-
-template <class P>
-__device__ __forceinline__ void get_step(const typename P::R* buf, int j, typename P::R (&ph)[3],
-                                         typename P::R (&pl)[3], typename P::R (&we)[3]) {
-    constexpr int NW = adj_state_words<P>();
-    const typename P::R* b = buf + (size_t)j * NW * kAdjBwdThreads;
-#pragma unroll
-    for (int x = 0; x < 3; ++x) {
-        ph[x] = b[x * kAdjBwdThreads];
-        we[x] = b[(3 + x) * kAdjBwdThreads];
-        pl[x] = NW == 9 ? b[(6 + x) * kAdjBwdThreads] : typename P::R(0);
-    }
-}
-
-template <class P>
-__global__ void __launch_bounds__(kAdjBwdThreads, adj_bwd_min_blocks<P>()) image_backward_kernel(const __grid_constant__ ImageArgs a) {
+__global__ void __launch_bounds__(kAdjThreads, adj_bwd_min_blocks<P>()) image_backward_kernel(const __grid_constant__ ImageArgs a) {
     using R = typename P::R;
-    extern __shared__ __align__(16) unsigned char s_dyn[];
-    R* s_seg = reinterpret_cast<R*>(s_dyn) + threadIdx.x;   // this thread's column of the segment buffer
     const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= a.n) return;
     MState<P> r;
@@ -792,20 +759,23 @@ __global__ void __launch_bounds__(kAdjBwdThreads, adj_bwd_min_blocks<P>()) image
     cc.base = kNone;
     typename AdjTypes<P>::Acc acc;
     acc.base = kNone;
+    // a segment's step inputs and their first two stage accelerations
+    MState<P> seg[kMaxCkptEvery];
+    R segA[kMaxCkptEvery][6];
     for (int s = (T + a.ckpt_every - 1) / a.ckpt_every - 1; s >= 0; --s) {
         load_state<P>(a, s, slot, r);
         const int j0 = s * a.ckpt_every;
         const int m = min(a.ckpt_every, T - j0);
-        // recompute the segment from its checkpoint (bitwise the forward's
-        // steps), keeping each step's input, then run its adjoint in reverse
+        // (the interior fast path does not pay here: the backward is
+        // latency-bound, and the second code path costs it registers)
         for (int j = 0; j < m; ++j) {
-            put_step<P>(s_seg, j, r);
-            model_step<P>(a, r, cc);
+            seg[j] = r;
+            model_step<P>(a, r, cc, &segA[j][0], &segA[j][3]);
         }
         for (int j = m - 1; j >= 0; --j) {
-            R ph[3], pl[3], we[3];
-            get_step<P>(s_seg, j, ph, pl, we);
-            model_step_adjoint<P>(a, ph, pl, we, lp, lw, cc, acc);
+            const R A1[3] = {segA[j][0], segA[j][1], segA[j][2]};
+            const R A2[3] = {segA[j][3], segA[j][4], segA[j][5]};
+            model_step_adjoint<P>(a, seg[j], A1, A2, lp, lw, cc, acc);
         }
     }
     flush(a, acc);
@@ -1024,10 +994,7 @@ static int image_backward_impl(const SlothGridDesc* g, const void* grid, const S
     fill_image_args(a, g, grid, p, nullptr, n, w.perm, w.ckpt, w.nsteps);
     a.image = const_cast<typename P::R*>(image_grad);
     a.ggrad = grid_grad;
-    const size_t smem = (size_t)p->ckpt_every * adj_state_words<P>() * sizeof(typename P::R) * kAdjBwdThreads;
-    e = cudaFuncSetAttribute(image_backward_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_status(e);
-    image_backward_kernel<P><<<(unsigned)((n + kAdjBwdThreads - 1) / kAdjBwdThreads), kAdjBwdThreads, smem, s>>>(a);
+    image_backward_kernel<P><<<(unsigned)((n + kAdjThreads - 1) / kAdjThreads), kAdjThreads, 0, s>>>(a);
     note_launch();
     return cuda_status(cudaGetLastError());
 }

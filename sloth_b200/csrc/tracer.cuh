@@ -778,6 +778,8 @@ __device__ __forceinline__ void rk4_step(const TraceArgs& a, Ray<P>& r, Cache& c
 template <int IB, int MODE, bool UNIT, int NK>
 __device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, CellPolyF2<NK>& cc, float phi) {
     if constexpr (UNIT) phi = 1.0f;
+    auto mphi = [&](float x) { return UNIT ? x : __fmul_rn(phi, x); };
+    auto mphi2 = [&](float2 x) { return UNIT ? x : __fmul2_rn(bc2(phi), x); };
     const float hphi = 0.5f * phi, phi6 = phi * (1.0f / 6.0f), phi2_6 = phi * phi6;
     const float S0 = a.Sf[0];
     const float2 S12 = make_float2(a.Sf[1], a.Sf[2]);
@@ -823,8 +825,8 @@ __device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
         sAyz = __fadd2_rn(sAyz, Ayz);
         sWx = __fmaf_rn(2.0f, Ax, sWx);
         sWyz = __ffma2_rn(two2, Ayz, sWyz);
-        stx = __fmaf_rn(phi, w3x, plx);
-        styz = __ffma2_rn(bc2(phi), w3yz, plyz);
+        stx = __fadd_rn(plx, mphi(w3x));
+        styz = __fadd2_rn(plyz, mphi2(w3yz));
     }
     g = __fmaf_rn(2.0f, s.n1, g);
     kq = __fmaf_rn(2.0f, s.k, kq);
@@ -835,13 +837,17 @@ __device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
     g = __fadd_rn(g, s.n1);
     kq = __fadd_rn(kq, s.k);
     // x: the scalar update
-    r.p[0].add(__fmaf_rn(phi, r.w[0].hi(), __fmaf_rn(phi, r.w[0].lo(), __fmul_rn(phi2_6, sAx))));
+    if constexpr (UNIT)
+        r.p[0].add(__fadd_rn(r.w[0].hi(), __fadd_rn(r.w[0].lo(), __fmul_rn(phi2_6, sAx))));
+    else
+        r.p[0].add(__fmaf_rn(phi, r.w[0].hi(), __fmaf_rn(phi, r.w[0].lo(), __fmul_rn(phi2_6, sAx))));
     r.w[0].add(__fmul_rn(phi6, sWx));
     // y, z: the same update on pairs
     {
         const float2 phi2 = bc2(phi);
         const float2 whi = make_float2(r.w[1].s, r.w[2].s), wlo = make_float2(r.w[1].c, r.w[2].c);
-        const float2 dp = __ffma2_rn(phi2, whi, __ffma2_rn(phi2, wlo, __fmul2_rn(bc2(phi2_6), sAyz)));
+        const float2 dp = UNIT ? __fadd2_rn(whi, __fadd2_rn(wlo, __fmul2_rn(bc2(phi2_6), sAyz)))
+                               : __ffma2_rn(phi2, whi, __ffma2_rn(phi2, wlo, __fmul2_rn(bc2(phi2_6), sAyz)));
         float2 ps = phyz, pc = plyz;
         kahan2(ps, pc, dp);
         r.p[1].s = ps.x; r.p[2].s = ps.y; r.p[1].c = pc.x; r.p[2].c = pc.y;
@@ -849,8 +855,8 @@ __device__ __forceinline__ void rk4_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
         kahan2(ws, wc, __fmul2_rn(bc2(phi6), sWyz));
         r.w[1].s = ws.x; r.w[2].s = ws.y; r.w[1].c = wc.x; r.w[2].c = wc.y;
     }
-    r.ph += (double)__fmul_rn(phi, g);
-    if constexpr (IB != IB_OFF) r.tau.add(__fmul_rn(phi, kq));
+    r.ph += (double)mphi(g);
+    if constexpr (IB != IB_OFF) r.tau.add(mphi(kq));
 }
 
 // One step: the paired FP32 form with the paired cell cache, the generic form

@@ -33,7 +33,8 @@ def test_sloth_arm_line():
     r = d["roofline"]
     for k in ("bound", "achieved", "peak", "unit", "frac", "traffic"):
         assert k in r, k
-    assert r["bound"] == "hbm" and r["unit"] == "GB/s" and r["achieved"] > 0 and r["peak"] > 0
+    assert r["bound"] == "fp32_pipe" and r["achieved"] > 0 and r["peak"] > 0 and 0 < r["frac"] < 1.5
+    assert r["hbm"]["peak_gbs"] > 0
     c = d["cpu_baseline"]
     assert c["value"] > 0 and c["cores"] >= 1 and c["kind"] in ("port", "reference") and c["sample"]
     e = d["e2e"]
@@ -44,6 +45,8 @@ def test_sloth_arm_line():
     assert d["adjoint"]["grad_vs_fd"]["max_abs_err_rel_to_max"] < 1e-2
     assert d["diagnostics"]["ms"] > 0
     assert d["fp32_vs_fp64"]["position_rel_L_max"] < 1e-6
+    assert d["config"]["field_samples_per_ray_step"] == 3 and d["rk4"]["field_samples_per_ray_step"] == 4
+    assert d["rk4"]["fp32_vs_fp64"]["position_rel_L_max"] < 1e-6
 
 
 def test_reference_arm_line():
