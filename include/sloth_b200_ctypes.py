@@ -3,7 +3,7 @@
 This is the binding a SLOTH maintainer adds beside src/core/propagator.py:
 SLOTH is pure Python, so its foreign-function interface is ctypes. It takes
 device pointers from any framework that exposes them (torch ``data_ptr()``,
-CuPy, DLPack) and declares only what a trace needs: the grid pack (K1), the
+CuPy, DLPack) and declares only what a trace needs: the grid pack (K1, trace layout), the
 workspace size, the FP32 / FP64 tracers and the error text. The structs
 mirror ``SlothGridDesc``, ``SlothTraceParams`` and ``SlothTraceOutputs`` field
 for field; the package's own binding (sloth_b200/_capi.py) covers the whole
@@ -40,8 +40,9 @@ class TraceOutputs(Structure):
 def load(path="libsloth_b200.so"):
     """Opens the library and declares the trace entry points' signatures."""
     lib = ctypes.CDLL(path)
-    lib.sloth_grid_pack_f32.restype = c_int
-    lib.sloth_grid_pack_f32.argtypes = [POINTER(GridDesc), c_void_p, c_int, c_double, c_void_p, c_void_p]
+    lib.sloth_grid_pack_trace_f32.restype = c_int
+    lib.sloth_grid_pack_trace_f32.argtypes = [POINTER(GridDesc), c_void_p, c_int, c_double, c_double, c_void_p,
+                                              c_void_p]
     lib.sloth_trace_workspace_bytes.restype = c_size_t
     lib.sloth_trace_workspace_bytes.argtypes = [c_int64]
     for name in ("sloth_trace_f32", "sloth_trace_f64"):
