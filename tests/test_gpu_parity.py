@@ -380,3 +380,19 @@ def test_smallest_grids(shape):
     assert far.mean() > 0.9
     assert np.abs(k32["phase"] - o["phase"])[:, far].max() <= 1e-6 * np.abs(o["phase"]).max()
     assert np.abs(k32["amp"].astype(np.float64) - o["amp"])[:, far].max() < 1e-6
+
+
+@pytest.mark.parametrize("precision,rtol", [("f64", 1e-12), ("f32", 1e-6)])
+@pytest.mark.parametrize("name", ["smooth_532", "dense_1064", "holes_532"])
+def test_trace_layout_phase_channel_matches_reference_phase(name, precision, rtol):
+    """K1's trace layout on the device, sampled by K0 at the golden points:
+    omega times the interpolated n - 1 channel is the legacy solver's own
+    ScalarDomain.phase (src/legacy/full_solver.py:342-345), 0 outside."""
+    g = golden("phase")
+    ne, pts, ref = g[f"{name}_ne"], g[f"{name}_points"], g[f"{name}_phase"]
+    ax = [g[f"{name}_{a}"] for a in "xyz"]
+    omega = float(g[f"{name}_omega"])
+    grid = runtime.pack_grid(torch.from_numpy(ne), [a[0] for a in ax], [a[1] - a[0] for a in ax], omega,
+                             precision=precision)
+    got = omega * runtime.sample(grid, pts)[0].cpu().numpy().astype(np.float64)
+    assert np.abs(got - ref).max() <= rtol * np.abs(ref).max()
