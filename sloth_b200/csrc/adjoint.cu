@@ -43,9 +43,19 @@
 namespace sloth {
 
 constexpr int kAdjThreads = 256;
-// The FP32 backward fits in 128 registers (two 256-thread CTAs per SM) with a
-// few bytes of spill; the FP64 one would spill kilobytes, so it keeps one.
-template <class P> constexpr int adj_bwd_min_blocks() { return sizeof(typename P::R) == 4 ? 2 : 1; }
+// The backward keeps the inputs of a checkpoint segment's steps in shared
+// memory, [step][word][thread] so that a warp's accesses are consecutive:
+// the position p and the velocity w per step, 6 words. In FP32 p is the
+// compensated sum's leading term alone; its compensation (below 1e-6 cells)
+// moves the point at which a stage is linearised, not the recomputed
+// trajectory. The first two stage accelerations of each step, which place
+// stages 2 and 3, stay in a per-thread array. 128 threads per CTA: a
+// 20-step segment takes 61 KB in FP32, so three CTAs share an SM (12 warps;
+// the kernel is latency-bound, and per-thread arrays of the whole state
+// spilled to DRAM at 16 warps).
+constexpr int kAdjBwdThreads = 128;
+constexpr int kAdjStateWords = 6;
+template <class P> constexpr int adj_bwd_min_blocks() { return sizeof(typename P::R) == 4 ? 3 : 1; }
 // The FP32 forward fits three 256-thread CTAs per SM (80 registers) without spilling.
 template <class P> constexpr int adj_fwd_min_blocks() { return sizeof(typename P::R) == 4 ? 3 : 1; }
 constexpr int kMaxCkptEvery = 32;
@@ -419,22 +429,18 @@ __device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const typename
         for (int c = 0; c < 8; ++c) acc.v[k][c] += gb[k] * w[c];
 }
 
-// Reverse of model_step from the step's input state r: (lp, lw) = adjoint of
-// the output (p', w') on entry, of the input (p, w) on return.
+// Reverse of model_step from the step's input (p = ph + pl, w = we) and its
+// first two stage accelerations A1, A2 (which place stages 2 and 3): (lp,
+// lw) = adjoint of the output (p', w') on entry, of the input (p, w) on
+// return.
 template <class P, class Cell, class Acc>
-__device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const MState<P>& r,
+__device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const typename P::R (&ph)[3],
+                                                   const typename P::R (&pl)[3], const typename P::R (&we)[3],
                                                    const typename P::R (&A1)[3], const typename P::R (&A2)[3],
                                                    typename P::R (&lp)[3], typename P::R (&lw)[3], Cell& cc,
                                                    Acc& acc) {
     using R = typename P::R;
-    R ph[3], pl[3], we[3], st[3];
-#pragma unroll
-    for (int x = 0; x < 3; ++x) {
-        ph[x] = r.p[x].hi();
-        pl[x] = r.p[x].lo();
-        we[x] = r.w[x].val();
-    }
-    // A1, A2 (which place stages 2 and 3) come from the segment's recompute.
+    R st[3];
     // Direct terms of p' = p + w + (A1 + 2 A2)/6, w' = w + (A1 + 4 A2 + A3)/6:
     R a1[3], a2[3], a3[3], pb[3], wb[3], q[3];
 #pragma unroll
@@ -724,9 +730,35 @@ __global__ void __launch_bounds__(kAdjThreads, adj_fwd_min_blocks<P>()) image_fo
     block_add((unsigned long long)t, &s_steps, a.total_steps);
 }
 
+// Input of step j of the current segment into / out of the shared buffer
+// (`buf` points at this thread's column).
 template <class P>
-__global__ void __launch_bounds__(kAdjThreads, adj_bwd_min_blocks<P>()) image_backward_kernel(const __grid_constant__ ImageArgs a) {
+__device__ __forceinline__ void put_step(typename P::R* buf, int j, const MState<P>& r) {
+    typename P::R* b = buf + (size_t)j * kAdjStateWords * kAdjBwdThreads;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        b[x * kAdjBwdThreads] = r.p[x].hi();
+        b[(3 + x) * kAdjBwdThreads] = r.w[x].val();
+    }
+}
+
+template <class P>
+__device__ __forceinline__ void get_step(const typename P::R* buf, int j, typename P::R (&ph)[3],
+                                         typename P::R (&pl)[3], typename P::R (&we)[3]) {
+    const typename P::R* b = buf + (size_t)j * kAdjStateWords * kAdjBwdThreads;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        ph[x] = b[x * kAdjBwdThreads];
+        we[x] = b[(3 + x) * kAdjBwdThreads];
+        pl[x] = typename P::R(0);
+    }
+}
+
+template <class P>
+__global__ void __launch_bounds__(kAdjBwdThreads, adj_bwd_min_blocks<P>()) image_backward_kernel(const __grid_constant__ ImageArgs a) {
     using R = typename P::R;
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    R* s_seg = reinterpret_cast<R*>(s_dyn) + threadIdx.x;   // this thread's column of the segment buffer
     const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= a.n) return;
     MState<P> r;
@@ -759,23 +791,23 @@ __global__ void __launch_bounds__(kAdjThreads, adj_bwd_min_blocks<P>()) image_ba
     cc.base = kNone;
     typename AdjTypes<P>::Acc acc;
     acc.base = kNone;
-    // a segment's step inputs and their first two stage accelerations
-    MState<P> seg[kMaxCkptEvery];
     R segA[kMaxCkptEvery][6];
     for (int s = (T + a.ckpt_every - 1) / a.ckpt_every - 1; s >= 0; --s) {
         load_state<P>(a, s, slot, r);
         const int j0 = s * a.ckpt_every;
         const int m = min(a.ckpt_every, T - j0);
-        // (the interior fast path does not pay here: the backward is
-        // latency-bound, and the second code path costs it registers)
+        // recompute the segment from its checkpoint (bitwise the forward's
+        // steps), keeping each step's input, then run its adjoint in reverse
         for (int j = 0; j < m; ++j) {
-            seg[j] = r;
+            put_step<P>(s_seg, j, r);
             model_step<P>(a, r, cc, &segA[j][0], &segA[j][3]);
         }
         for (int j = m - 1; j >= 0; --j) {
+            R ph[3], pl[3], we[3];
+            get_step<P>(s_seg, j, ph, pl, we);
             const R A1[3] = {segA[j][0], segA[j][1], segA[j][2]};
             const R A2[3] = {segA[j][3], segA[j][4], segA[j][5]};
-            model_step_adjoint<P>(a, seg[j], A1, A2, lp, lw, cc, acc);
+            model_step_adjoint<P>(a, ph, pl, we, A1, A2, lp, lw, cc, acc);
         }
     }
     flush(a, acc);
@@ -994,7 +1026,10 @@ static int image_backward_impl(const SlothGridDesc* g, const void* grid, const S
     fill_image_args(a, g, grid, p, nullptr, n, w.perm, w.ckpt, w.nsteps);
     a.image = const_cast<typename P::R*>(image_grad);
     a.ggrad = grid_grad;
-    image_backward_kernel<P><<<(unsigned)((n + kAdjThreads - 1) / kAdjThreads), kAdjThreads, 0, s>>>(a);
+    const size_t smem = (size_t)p->ckpt_every * kAdjStateWords * sizeof(typename P::R) * kAdjBwdThreads;
+    e = cudaFuncSetAttribute(image_backward_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e);
+    image_backward_kernel<P><<<(unsigned)((n + kAdjBwdThreads - 1) / kAdjBwdThreads), kAdjBwdThreads, smem, s>>>(a);
     note_launch();
     return cuda_status(cudaGetLastError());
 }
