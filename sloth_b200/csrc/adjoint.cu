@@ -310,6 +310,16 @@ constexpr unsigned kNone = 0xffffffffu;
 template <class P> struct AdjTypes { using Cell = GradCell<P>; using Acc = CornerAcc<P>; };
 template <> struct AdjTypes<PolF32> { using Cell = GradCellF2; using Acc = CornerAcc<PolF32>; };
 
+// Adds (x, y, z, w) to *p as one vector reduction that returns nothing
+// (red.global.add.v4.f32, sm_90 and later). A float4 atomicAdd compiles to
+// an atomic that sends each old value back through the crossbar; with about
+// one flush of eight corners per three ray-steps that return traffic cost
+// the backward 9% of its time.
+__device__ __forceinline__ void red_add_v4(float4* p, float x, float y, float z, float w) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};"
+                 :: "l"(p), "f"(x), "f"(y), "f"(z), "f"(w) : "memory");
+}
+
 template <class P>
 __device__ __forceinline__ void flush(const ImageArgs& a, CornerAcc<P>& acc) {
     using R = typename P::R;
@@ -321,7 +331,7 @@ __device__ __forceinline__ void flush(const ImageArgs& a, CornerAcc<P>& acc) {
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         if constexpr (sizeof(R) == 4) {
-            atomicAdd(reinterpret_cast<float4*>(a.ggrad) + off[c], make_float4(0.f, acc.v[0][c], acc.v[1][c], acc.v[2][c]));
+            red_add_v4(reinterpret_cast<float4*>(a.ggrad) + off[c], 0.0f, acc.v[0][c], acc.v[1][c], acc.v[2][c]);
         } else {
             double* d = reinterpret_cast<double*>(a.ggrad) + 4 * (size_t)off[c];
             atomicAdd(d + 1, acc.v[0][c]);
