@@ -110,8 +110,9 @@ def test_kolmogorov_128_with_absorption(precision, integ):
     assert (k["steps"] != o["steps"]).mean() < 1e-3
 
 
+@pytest.mark.parametrize("integ", ["rkn", "rk4"])
 @pytest.mark.parametrize("precision", ["f64", "f32"])
-def test_many_saves_inside_interior_runs(precision):
+def test_many_saves_inside_interior_runs(precision, integ):
     """40 saves, every few steps: the tracer's uniform step loop must stop at
     each save inside its interior runs. Against the oracle at every save."""
     n = 48
@@ -120,7 +121,7 @@ def test_many_saves_inside_interior_runs(precision):
     rays = workloads.gaussian_beam(3000, waist=1.5e-3, L=L, seed=42).numpy()
     sched = runtime.schedule_times(np.linspace(0.0, 1.2 * L, 40), (h, h, h))
     assert sched.n_saves == 40 and sched.save_every >= 2
-    kw = dict(inv_brems=True, Te=20.0, Z=1.0)
+    kw = dict(inv_brems=True, Te=20.0, Z=1.0, integrator=integ)
     k = run_kernel(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched, precision=precision, **kw)
     o = run_oracle(ne, rays, (-L / 2,) * 3, (h,) * 3, OMEGA, sched, **kw)
     assert position_error(k["state"], o["state"], L) < _tol(precision)

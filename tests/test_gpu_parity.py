@@ -224,9 +224,10 @@ def _noncubic_case(axis, nrays=2000, seed=3):
 
 
 @pytest.mark.parametrize("axis", [0, 1])
-def test_noncubic_anisotropic_grid(axis):
+@pytest.mark.parametrize("integ", ["rkn", "rk4"])
+def test_noncubic_anisotropic_grid(axis, integ):
     ne, rays, origin, h, omega, sched, ext = _noncubic_case(axis)
-    kw = dict(axis=axis, project=True, plane=ext[axis] / 2, inv_brems=True, Te=20.0, Z=1.0)
+    kw = dict(axis=axis, project=True, plane=ext[axis] / 2, inv_brems=True, Te=20.0, Z=1.0, integrator=integ)
     o = run_oracle(ne, rays, origin, h, omega, sched, **kw)
     k64 = run_kernel(ne, rays, origin, h, omega, sched, precision="f64", **kw)
     Lmax = max(ext)
@@ -245,8 +246,9 @@ def test_noncubic_anisotropic_grid(axis):
     assert np.abs(k32["amp"].astype(np.float64) - o["amp"])[:, far].max() < 1e-6
 
 
+@pytest.mark.parametrize("integ", ["rkn", "rk4"])
 @pytest.mark.parametrize("precision", ["f32", "f64"])
-def test_interior_fast_path_is_bitwise_identical(precision):
+def test_interior_fast_path_is_bitwise_identical(precision, integ):
     """With a known density range the tracer skips the per-stage grid test on
     interior steps, the face test on runs of steps proven interior, and the
     warp's per-step bookkeeping while all its rays are on such a run. It takes
@@ -263,7 +265,7 @@ def test_interior_fast_path_is_bitwise_identical(precision):
     assert g.q_min <= 0.0 < g.q_max
     dt = torch.float32 if precision == "f32" else torch.float64
     r = torch.from_numpy(rays).to("cuda", dt)
-    kw = dict(project=True, plane=L / 2, inv_brems=True, Te=20.0, Z=1.0, want_state=True)
+    kw = dict(project=True, plane=L / 2, inv_brems=True, Te=20.0, Z=1.0, want_state=True, integrator=integ)
     fast = runtime.trace(g, r, sched, **kw)
     slow = runtime.trace(dataclasses.replace(g, q_min=float("inf")), r, sched, **kw)
     torch.cuda.synchronize()
