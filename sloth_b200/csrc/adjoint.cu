@@ -308,7 +308,8 @@ struct CornerAcc {
 constexpr unsigned kNone = 0xffffffffu;
 
 template <class P> struct AdjTypes { using Cell = GradCell<P>; using Acc = CornerAcc<P>; };
-template <> struct AdjTypes<PolF32> { using Cell = GradCellF2; using Acc = CornerAcc<PolF32>; };
+struct CornerAccF2;
+template <> struct AdjTypes<PolF32> { using Cell = GradCellF2; using Acc = CornerAccF2; };
 
 // Adds (x, y, z, w) to *p as one vector reduction that returns nothing
 // (red.global.add.v4.f32, sm_90 and later). A float4 atomicAdd compiles to
@@ -342,12 +343,35 @@ __device__ __forceinline__ void flush(const ImageArgs& a, CornerAcc<P>& acc) {
     acc.base = kNone;
 }
 
-// Stage adjoint on the paired FP32 cache with scalar arithmetic (the backward
-// is latency-bound: paired instructions did not shorten it).
+// FP32 corner sums as pairs: v[k][i] holds channel k + 1 at corners 2i and
+// 2i + 1, which differ in z only, so that a pair is one sm_100 paired FP32
+// operation and one pair of adjacent voxels in the flush.
+struct CornerAccF2 {
+    unsigned base;
+    float2 v[3][4];
+};
+
+__device__ __forceinline__ void flush(const ImageArgs& a, CornerAccF2& acc) {
+    if (acc.base == kNone) return;
+    const GridGeo& g = a.geo;
+    const unsigned b = acc.base;
+    const unsigned off[4] = {b, b + g.sy, b + g.sx, b + g.sx + g.sy};
+    float4* gg = reinterpret_cast<float4*>(a.ggrad);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        red_add_v4(gg + off[i], 0.0f, acc.v[0][i].x, acc.v[1][i].x, acc.v[2][i].x);
+        red_add_v4(gg + off[i] + 1u, 0.0f, acc.v[0][i].y, acc.v[1][i].y, acc.v[2][i].y);
+    }
+    acc.base = kNone;
+}
+
+// Stage adjoint on the paired FP32 cache: channels 2 and 3 of the Jacobian
+// transpose, the corner weights and the corner sums run as paired FP32
+// operations (__ffma2_rn / __fmul2_rn), channel 1 scalar.
 template <class P>
 __device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const float (&hi)[3], const float (&lo)[3],
                                               const float (&Abar)[3], float (&q)[3], GradCellF2& cc,
-                                              CornerAcc<PolF32>& acc) {
+                                              CornerAccF2& acc) {
     unsigned b;
     float f[3];
     if (!locate<P>(a.geo, hi, lo, b, f)) {
@@ -356,38 +380,45 @@ __device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const float (&
     }
     load_cell_f2(a, b, cc);
     const float fx = f[0], fy = f[1], fz = f[2];
+    const float2 fx2 = make_float2(fx, fx), fy2 = make_float2(fy, fy), fz2 = make_float2(fz, fz);
     float gb[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) gb[k] = (float)a.S[k] * Abar[k];
-    q[0] = q[1] = q[2] = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        // channel k + 1 of the voxel: pair k == 0 ? 0 : 1, half k == 0 ? y : (k == 1 ? x : y)
-        float t[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) t[i] = k == 0 ? cc.t[0][i].y : (k == 1 ? cc.t[1][i].x : cc.t[1][i].y);
-        const float dx = (t[1] + fy * t[4]) + fz * (t[5] + fy * t[7]);
-        const float dy = (t[2] + fx * t[4]) + fz * (t[6] + fx * t[7]);
-        const float dz = (t[3] + fx * t[5]) + fy * (t[6] + fx * t[7]);
-        q[0] += gb[k] * dx;
-        q[1] += gb[k] * dy;
-        q[2] += gb[k] * dz;
-    }
+    // J^T gb. Channel 1 (dq/du) is the .y half of pair 0, channels 2 and 3 are pair 1.
+    const float2* t0 = cc.t[0];
+    const float2* t1 = cc.t[1];
+    const float u76 = fmaf(fx, t0[7].y, t0[6].y);
+    const float d1x = fmaf(fz, fmaf(fy, t0[7].y, t0[5].y), fmaf(fy, t0[4].y, t0[1].y));
+    const float d1y = fmaf(fz, u76, fmaf(fx, t0[4].y, t0[2].y));
+    const float d1z = fmaf(fy, u76, fmaf(fx, t0[5].y, t0[3].y));
+    const float2 v76 = __ffma2_rn(fx2, t1[7], t1[6]);
+    const float2 d2x = __ffma2_rn(fz2, __ffma2_rn(fy2, t1[7], t1[5]), __ffma2_rn(fy2, t1[4], t1[1]));
+    const float2 d2y = __ffma2_rn(fz2, v76, __ffma2_rn(fx2, t1[4], t1[2]));
+    const float2 d2z = __ffma2_rn(fy2, v76, __ffma2_rn(fx2, t1[5], t1[3]));
+    q[0] = fmaf(gb[2], d2x.y, fmaf(gb[1], d2x.x, gb[0] * d1x));
+    q[1] = fmaf(gb[2], d2y.y, fmaf(gb[1], d2y.x, gb[0] * d1y));
+    q[2] = fmaf(gb[2], d2z.y, fmaf(gb[1], d2z.x, gb[0] * d1z));
     if (b != acc.base) {
         flush(a, acc);
         acc.base = b;
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
-            for (int c = 0; c < 8; ++c) acc.v[k][c] = 0.0f;
+            for (int i = 0; i < 4; ++i) acc.v[k][i] = make_float2(0.0f, 0.0f);
     }
-    const float ex = 1.0f - fx, ey = 1.0f - fy, ez = 1.0f - fz;
-    const float w00 = ex * ey, w01 = ex * fy, w10 = fx * ey, w11 = fx * fy;
-    const float w[8] = {w00 * ez, w00 * fz, w01 * ez, w01 * fz, w10 * ez, w10 * fz, w11 * ez, w11 * fz};
+    // corner weights: pair i = (corner 2i, 2i + 1) = X * Y * (1 - fz, fz) with
+    // X = 1 - fx or fx (i >> 1), Y = 1 - fy or fy (i & 1)
+    const float2 one = make_float2(1.0f, 1.0f), neg = make_float2(-1.0f, -1.0f);
+    const float2 ex2 = __ffma2_rn(fx2, neg, one), ey2 = __ffma2_rn(fy2, neg, one);
+    const float2 zz = __ffma2_rn(fz2, make_float2(-1.0f, 1.0f), make_float2(1.0f, 0.0f));
+    const float2 xz0 = __fmul2_rn(ex2, zz), xz1 = __fmul2_rn(fx2, zz);
+    const float2 w[4] = {__fmul2_rn(xz0, ey2), __fmul2_rn(xz0, fy2), __fmul2_rn(xz1, ey2), __fmul2_rn(xz1, fy2)};
 #pragma unroll
-    for (int k = 0; k < 3; ++k)
+    for (int k = 0; k < 3; ++k) {
+        const float2 g2 = make_float2(gb[k], gb[k]);
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc.v[k][c] += gb[k] * w[c];
+        for (int i = 0; i < 4; ++i) acc.v[k][i] = __ffma2_rn(g2, w[i], acc.v[k][i]);
+    }
 }
 
 // Stage adjoint: with Abar = d L / d(stage acceleration), adds
@@ -812,11 +843,19 @@ __global__ void __launch_bounds__(kAdjBwdThreads, adj_bwd_min_blocks<P>()) image
             put_step<P>(s_seg, j, r);
             model_step<P>(a, r, cc, &segA[j][0], &segA[j][3]);
         }
+        // segA lives in local memory, mostly in L2: step j - 1's accelerations
+        // are loaded while step j's adjoint runs
+        R An[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) An[k] = segA[m - 1][k];
         for (int j = m - 1; j >= 0; --j) {
             R ph[3], pl[3], we[3];
             get_step<P>(s_seg, j, ph, pl, we);
-            const R A1[3] = {segA[j][0], segA[j][1], segA[j][2]};
-            const R A2[3] = {segA[j][3], segA[j][4], segA[j][5]};
+            const R A1[3] = {An[0], An[1], An[2]};
+            const R A2[3] = {An[3], An[4], An[5]};
+            const int jn = j > 0 ? j - 1 : 0;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) An[k] = segA[jn][k];
             model_step_adjoint<P>(a, ph, pl, we, A1, A2, lp, lw, cc, acc);
         }
     }
