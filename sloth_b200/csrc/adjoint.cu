@@ -43,19 +43,21 @@
 namespace sloth {
 
 constexpr int kAdjThreads = 256;
-// The backward keeps the inputs of a checkpoint segment's steps in shared
-// memory, [step][word][thread] so that a warp's accesses are consecutive:
-// the position p and the velocity w per step, 6 words. In FP32 p is the
-// compensated sum's leading term alone; its compensation (below 1e-6 cells)
-// moves the point at which a stage is linearised, not the recomputed
-// trajectory. The first two stage accelerations of each step, which place
-// stages 2 and 3, stay in a per-thread array. 128 threads per CTA: a
-// 20-step segment takes 61 KB in FP32, so three CTAs share an SM (12 warps;
-// the kernel is latency-bound, and per-thread arrays of the whole state
-// spilled to DRAM at 16 warps).
+// The backward's recompute of a checkpoint segment records where each stage
+// of each step sampled the field (its cell and in-cell coordinates), and the
+// step adjoints linearise there. Stages 1 and 2's in-cell coordinates go to
+// shared memory, [step][word][thread] so that a warp's accesses are
+// consecutive (5 words per step); the three cells and the other in-cell
+// coordinates stay in a per-thread array. 128 threads per CTA: a 20-step
+// segment takes 51 KB of shared memory in FP32, so four CTAs share an SM
+// (16 warps; the kernel is latency-bound).
 constexpr int kAdjBwdThreads = 128;
-constexpr int kAdjStateWords = 6;
-template <class P> constexpr int adj_bwd_min_blocks() { return sizeof(typename P::R) == 4 ? 3 : 1; }
+constexpr int kAdjStateWords = 5;
+// Two FP32 builds of the backward: four CTAs per SM (128 registers) when
+// four segment buffers fit an SM's shared memory (checkpoints at most every
+// 21 steps), three (150 registers) otherwise. FP64 runs one CTA per SM.
+constexpr int kAdjBwdSmemPerSm = 228 * 1024;   // shared memory per SM
+constexpr int kAdjBwdSmemPerCta = 1024;        // reserved by the system per CTA
 // The FP32 forward fits three 256-thread CTAs per SM (80 registers) without spilling.
 template <class P> constexpr int adj_fwd_min_blocks() { return sizeof(typename P::R) == 4 ? 3 : 1; }
 constexpr int kMaxCkptEvery = 32;
@@ -233,16 +235,39 @@ __device__ __forceinline__ void load_cell(const ImageArgs& a, unsigned b, GradCe
     poly_coeffs<R>(cc.t[2], v0.w, v1.w, v2.w, v3.w, v4.w, v5.w, v6.w, v7.w);
 }
 
-// Acceleration S * grad(q) at hi + lo (zero outside).
+// Where one stage sampled the field: the cell (kNone when the point was
+// outside the grid, fill 0) and the in-cell coordinates. The backward's
+// recompute records the three stages of every step, and the step's adjoint
+// linearises at exactly those points.
+constexpr unsigned kNone = 0xffffffffu;
+
+template <class P>
+struct StageRec {
+    unsigned b;
+    typename P::R f[3];
+};
+
+// Acceleration S * grad(q) at hi + lo (zero outside); with rec, where it
+// sampled.
 template <class P, bool INTERIOR, class Cell>
 __device__ __forceinline__ void accel(const ImageArgs& a, const typename P::R (&hi)[3], const typename P::R (&lo)[3],
-                                      typename P::R (&A)[3], Cell& cc) {
+                                      typename P::R (&A)[3], Cell& cc, StageRec<P>* rec = nullptr) {
     using R = typename P::R;
     unsigned b;
     R f[3];
     if (!locate<P, INTERIOR>(a.geo, hi, lo, b, f)) {
         A[0] = A[1] = A[2] = R(0);
+        if (rec) {
+            rec->b = kNone;
+            rec->f[0] = rec->f[1] = rec->f[2] = R(0);
+        }
         return;
+    }
+    if (rec) {
+        rec->b = b;
+        rec->f[0] = f[0];
+        rec->f[1] = f[1];
+        rec->f[2] = f[2];
     }
     if constexpr (std::is_same<Cell, GradCellF2>::value) {
         load_cell_f2(a, b, cc);
@@ -263,8 +288,7 @@ __device__ __forceinline__ void accel(const ImageArgs& a, const typename P::R (&
 //   p' = p + w + (A1 + 2 A2)/6,  w' = w + (A1 + 4 A2 + A3)/6,
 //   stages at p, p + w/2 + A1/8, p + w + A2/2.
 template <class P, bool INTERIOR = false, class Cell>
-__device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, Cell& cc,
-                                           typename P::R* A1out = nullptr, typename P::R* A2out = nullptr) {
+__device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, Cell& cc, StageRec<P>* rec = nullptr) {
     using R = typename P::R;
     R ph[3], pl[3], we[3], st[3], A1[3], A2[3], A3[3];
 #pragma unroll
@@ -273,20 +297,13 @@ __device__ __forceinline__ void model_step(const ImageArgs& a, MState<P>& r, Cel
         pl[x] = r.p[x].lo();
         we[x] = r.w[x].val();
     }
-    accel<P, INTERIOR>(a, ph, pl, A1, cc);
+    accel<P, INTERIOR>(a, ph, pl, A1, cc, rec);
 #pragma unroll
     for (int x = 0; x < 3; ++x) st[x] = pl[x] + (R(0.5) * we[x] + R(0.125) * A1[x]);
-    accel<P, INTERIOR>(a, ph, st, A2, cc);
+    accel<P, INTERIOR>(a, ph, st, A2, cc, rec ? rec + 1 : nullptr);
 #pragma unroll
     for (int x = 0; x < 3; ++x) st[x] = pl[x] + (we[x] + R(0.5) * A2[x]);
-    accel<P, INTERIOR>(a, ph, st, A3, cc);
-    if (A1out) {
-#pragma unroll
-        for (int x = 0; x < 3; ++x) {
-            A1out[x] = A1[x];
-            A2out[x] = A2[x];
-        }
-    }
+    accel<P, INTERIOR>(a, ph, st, A3, cc, rec ? rec + 2 : nullptr);
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         const R sA = A1[x] + R(2) * A2[x];
@@ -304,8 +321,6 @@ struct CornerAcc {
     unsigned base;               // cell of the pending sums (kNone: none)
     typename P::R v[3][8];       // d L / d(channel k) at corner c
 };
-
-constexpr unsigned kNone = 0xffffffffu;
 
 template <class P> struct AdjTypes { using Cell = GradCell<P>; using Acc = CornerAcc<P>; };
 struct CornerAccF2;
@@ -369,15 +384,15 @@ __device__ __forceinline__ void flush(const ImageArgs& a, CornerAccF2& acc) {
 // transpose, the corner weights and the corner sums run as paired FP32
 // operations (__ffma2_rn / __fmul2_rn), channel 1 scalar.
 template <class P>
-__device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const float (&hi)[3], const float (&lo)[3],
+__device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const StageRec<PolF32>& rec,
                                               const float (&Abar)[3], float (&q)[3], GradCellF2& cc,
                                               CornerAccF2& acc) {
-    unsigned b;
-    float f[3];
-    if (!locate<P>(a.geo, hi, lo, b, f)) {
+    const unsigned b = rec.b;
+    if (b == kNone) {
         q[0] = q[1] = q[2] = 0.0f;
         return;
     }
+    const float f[3] = {rec.f[0], rec.f[1], rec.f[2]};
     load_cell_f2(a, b, cc);
     const float fx = f[0], fy = f[1], fz = f[2];
     const float2 fx2 = make_float2(fx, fx), fy2 = make_float2(fy, fy), fz2 = make_float2(fz, fz);
@@ -425,16 +440,16 @@ __device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const float (&
 // Abar_k * S_k * (corner weight) to the corners of the stage's cell and
 // returns q = J^T (S * Abar), J = d grad(q) / d p at the stage point.
 template <class P>
-__device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const typename P::R (&hi)[3],
-                                              const typename P::R (&lo)[3], const typename P::R (&Abar)[3],
-                                              typename P::R (&q)[3], GradCell<P>& cc, CornerAcc<P>& acc) {
+__device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const StageRec<P>& rec,
+                                              const typename P::R (&Abar)[3], typename P::R (&q)[3],
+                                              GradCell<P>& cc, CornerAcc<P>& acc) {
     using R = typename P::R;
-    unsigned b;
-    R f[3];
-    if (!locate<P>(a.geo, hi, lo, b, f)) {
+    const unsigned b = rec.b;
+    if (b == kNone) {
         q[0] = q[1] = q[2] = R(0);
         return;
     }
+    const R f[3] = {rec.f[0], rec.f[1], rec.f[2]};
     load_cell<P>(a, b, cc);
     const R fx = f[0], fy = f[1], fz = f[2];
     R gb[3];
@@ -470,18 +485,16 @@ __device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const typename
         for (int c = 0; c < 8; ++c) acc.v[k][c] += gb[k] * w[c];
 }
 
-// Reverse of model_step from the step's input (p = ph + pl, w = we) and its
-// first two stage accelerations A1, A2 (which place stages 2 and 3): (lp,
-// lw) = adjoint of the output (p', w') on entry, of the input (p, w) on
-// return.
+// Reverse of model_step from where its three stages sampled the field (the
+// records of the recompute): (lp, lw) = adjoint of the output (p', w') on
+// entry, of the input (p, w) on return. The step's stage points are
+// p, p + w/2 + A1/8 and p + w + A2/2, so the chain through them needs only
+// each stage's Jacobian transpose, not the step's p or w.
 template <class P, class Cell, class Acc>
-__device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const typename P::R (&ph)[3],
-                                                   const typename P::R (&pl)[3], const typename P::R (&we)[3],
-                                                   const typename P::R (&A1)[3], const typename P::R (&A2)[3],
+__device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const StageRec<P> (&rec)[3],
                                                    typename P::R (&lp)[3], typename P::R (&lw)[3], Cell& cc,
                                                    Acc& acc) {
     using R = typename P::R;
-    R st[3];
     // Direct terms of p' = p + w + (A1 + 2 A2)/6, w' = w + (A1 + 4 A2 + A3)/6:
     R a1[3], a2[3], a3[3], pb[3], wb[3], q[3];
 #pragma unroll
@@ -493,9 +506,7 @@ __device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const typ
         wb[x] = lp[x] + lw[x];
     }
     // stage 3 at p + w + A2/2
-#pragma unroll
-    for (int x = 0; x < 3; ++x) st[x] = pl[x] + (we[x] + R(0.5) * A2[x]);
-    stage_adjoint<P>(a, ph, st, a3, q, cc, acc);
+    stage_adjoint<P>(a, rec[2], a3, q, cc, acc);
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         pb[x] += q[x];
@@ -503,9 +514,7 @@ __device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const typ
         a2[x] += R(0.5) * q[x];
     }
     // stage 2 at p + w/2 + A1/8
-#pragma unroll
-    for (int x = 0; x < 3; ++x) st[x] = pl[x] + (R(0.5) * we[x] + R(0.125) * A1[x]);
-    stage_adjoint<P>(a, ph, st, a2, q, cc, acc);
+    stage_adjoint<P>(a, rec[1], a2, q, cc, acc);
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         pb[x] += q[x];
@@ -513,7 +522,7 @@ __device__ __forceinline__ void model_step_adjoint(const ImageArgs& a, const typ
         a1[x] += R(0.125) * q[x];
     }
     // stage 1 at p
-    stage_adjoint<P>(a, ph, pl, a1, q, cc, acc);
+    stage_adjoint<P>(a, rec[0], a1, q, cc, acc);
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         lp[x] = pb[x] + q[x];
@@ -771,32 +780,29 @@ __global__ void __launch_bounds__(kAdjThreads, adj_fwd_min_blocks<P>()) image_fo
     block_add((unsigned long long)t, &s_steps, a.total_steps);
 }
 
-// Input of step j of the current segment into / out of the shared buffer
-// (`buf` points at this thread's column).
+// In-cell coordinates of stage 1 and the first two of stage 2 of step j of
+// the current segment into / out of the shared buffer (`buf` points at this
+// thread's column).
 template <class P>
-__device__ __forceinline__ void put_step(typename P::R* buf, int j, const MState<P>& r) {
+__device__ __forceinline__ void put_step(typename P::R* buf, int j, const StageRec<P> (&rec)[3]) {
     typename P::R* b = buf + (size_t)j * kAdjStateWords * kAdjBwdThreads;
 #pragma unroll
-    for (int x = 0; x < 3; ++x) {
-        b[x * kAdjBwdThreads] = r.p[x].hi();
-        b[(3 + x) * kAdjBwdThreads] = r.w[x].val();
-    }
+    for (int x = 0; x < 3; ++x) b[x * kAdjBwdThreads] = rec[0].f[x];
+    b[3 * kAdjBwdThreads] = rec[1].f[0];
+    b[4 * kAdjBwdThreads] = rec[1].f[1];
 }
 
 template <class P>
-__device__ __forceinline__ void get_step(const typename P::R* buf, int j, typename P::R (&ph)[3],
-                                         typename P::R (&pl)[3], typename P::R (&we)[3]) {
+__device__ __forceinline__ void get_step(const typename P::R* buf, int j, StageRec<P> (&rec)[3]) {
     const typename P::R* b = buf + (size_t)j * kAdjStateWords * kAdjBwdThreads;
 #pragma unroll
-    for (int x = 0; x < 3; ++x) {
-        ph[x] = b[x * kAdjBwdThreads];
-        we[x] = b[(3 + x) * kAdjBwdThreads];
-        pl[x] = typename P::R(0);
-    }
+    for (int x = 0; x < 3; ++x) rec[0].f[x] = b[x * kAdjBwdThreads];
+    rec[1].f[0] = b[3 * kAdjBwdThreads];
+    rec[1].f[1] = b[4 * kAdjBwdThreads];
 }
 
-template <class P>
-__global__ void __launch_bounds__(kAdjBwdThreads, adj_bwd_min_blocks<P>()) image_backward_kernel(const __grid_constant__ ImageArgs a) {
+template <class P, int MINB>
+__global__ void __launch_bounds__(kAdjBwdThreads, MINB) image_backward_kernel(const __grid_constant__ ImageArgs a) {
     using R = typename P::R;
     extern __shared__ __align__(16) unsigned char s_dyn[];
     R* s_seg = reinterpret_cast<R*>(s_dyn) + threadIdx.x;   // this thread's column of the segment buffer
@@ -832,31 +838,51 @@ __global__ void __launch_bounds__(kAdjBwdThreads, adj_bwd_min_blocks<P>()) image
     cc.base = kNone;
     typename AdjTypes<P>::Acc acc;
     acc.base = kNone;
-    R segA[kMaxCkptEvery][6];
+    // the three stage cells and the in-cell coordinates that the shared
+    // buffer does not hold (stage 2's third, stage 3's) of each step
+    unsigned segB[kMaxCkptEvery][3];
+    R segF[kMaxCkptEvery][4];
     for (int s = (T + a.ckpt_every - 1) / a.ckpt_every - 1; s >= 0; --s) {
         load_state<P>(a, s, slot, r);
         const int j0 = s * a.ckpt_every;
         const int m = min(a.ckpt_every, T - j0);
         // recompute the segment from its checkpoint (bitwise the forward's
-        // steps), keeping each step's input, then run its adjoint in reverse
+        // steps), recording where each stage sampled, then run its adjoint
+        // in reverse
         for (int j = 0; j < m; ++j) {
-            put_step<P>(s_seg, j, r);
-            model_step<P>(a, r, cc, &segA[j][0], &segA[j][3]);
-        }
-        // segA lives in local memory, mostly in L2: step j - 1's accelerations
-        // are loaded while step j's adjoint runs
-        R An[6];
+            StageRec<P> rec[3];
+            model_step<P>(a, r, cc, rec);
+            put_step<P>(s_seg, j, rec);
 #pragma unroll
-        for (int k = 0; k < 6; ++k) An[k] = segA[m - 1][k];
+            for (int k = 0; k < 3; ++k) {
+                segB[j][k] = rec[k].b;
+                segF[j][k] = rec[2].f[k];
+            }
+            segF[j][3] = rec[1].f[2];
+        }
+        // segB / segF live in local memory, mostly in L2: step j - 1's
+        // records are loaded while step j's adjoint runs
+        unsigned Bn[3];
+        R Fn[4];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) Bn[k] = segB[m - 1][k];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) Fn[k] = segF[m - 1][k];
         for (int j = m - 1; j >= 0; --j) {
-            R ph[3], pl[3], we[3];
-            get_step<P>(s_seg, j, ph, pl, we);
-            const R A1[3] = {An[0], An[1], An[2]};
-            const R A2[3] = {An[3], An[4], An[5]};
+            StageRec<P> rec[3];
+            get_step<P>(s_seg, j, rec);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                rec[k].b = Bn[k];
+                rec[2].f[k] = Fn[k];
+            }
+            rec[1].f[2] = Fn[3];
             const int jn = j > 0 ? j - 1 : 0;
 #pragma unroll
-            for (int k = 0; k < 6; ++k) An[k] = segA[jn][k];
-            model_step_adjoint<P>(a, ph, pl, we, A1, A2, lp, lw, cc, acc);
+            for (int k = 0; k < 3; ++k) Bn[k] = segB[jn][k];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) Fn[k] = segF[jn][k];
+            model_step_adjoint<P>(a, rec, lp, lw, cc, acc);
         }
     }
     flush(a, acc);
@@ -1076,9 +1102,21 @@ static int image_backward_impl(const SlothGridDesc* g, const void* grid, const S
     a.image = const_cast<typename P::R*>(image_grad);
     a.ggrad = grid_grad;
     const size_t smem = (size_t)p->ckpt_every * kAdjStateWords * sizeof(typename P::R) * kAdjBwdThreads;
-    e = cudaFuncSetAttribute(image_backward_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const unsigned blocks = (unsigned)((n + kAdjBwdThreads - 1) / kAdjBwdThreads);
+    auto launch = [&](auto kernel) {
+        cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err == cudaSuccess) kernel<<<blocks, kAdjBwdThreads, smem, s>>>(a);
+        return err;
+    };
+    if constexpr (sizeof(typename P::R) == 4) {
+        if (4 * (smem + kAdjBwdSmemPerCta) <= (size_t)kAdjBwdSmemPerSm)
+            e = launch(image_backward_kernel<P, 4>);
+        else
+            e = launch(image_backward_kernel<P, 3>);
+    } else {
+        e = launch(image_backward_kernel<P, 1>);
+    }
     if (e != cudaSuccess) return cuda_status(e);
-    image_backward_kernel<P><<<(unsigned)((n + kAdjBwdThreads - 1) / kAdjBwdThreads), kAdjBwdThreads, smem, s>>>(a);
     note_launch();
     return cuda_status(cudaGetLastError());
 }
