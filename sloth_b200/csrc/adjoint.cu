@@ -1065,9 +1065,14 @@ static int image_forward_impl(const SlothGridDesc* g, const void* grid, const Sl
     if (e != cudaSuccess) return cuda_status(e);
     if (n == 0) return SLOTH_OK;
     ImageWs w = carve(ws, p, n);
-    const int bbits = bucket_bits_for(n);
+    // One thread per ray in bucket order, with no tile sort: buckets of one
+    // transverse entry cell each (for grids of up to 513 points across the
+    // probing axis) keep a warp's rays in few cells, so that its cell loads
+    // and gradient flushes share addresses.
+    const int bbits = kMaxBucketBits;
     if ((e = cudaMemsetAsync(w.hist, 0, (size_t)4 << bbits, s)) != cudaSuccess) return cuda_status(e);
-    rc = launch_prepass<typename P::R>(g, p->probing_axis, rays, n, bbits, w.keys, w.hist, w.perm, w.skeys, sms, s);
+    rc = launch_prepass<typename P::R>(g, p->probing_axis, rays, n, bbits, w.keys, w.hist, w.perm, w.skeys, sms, s,
+                                       true);
     if (rc) return rc;
     ImageArgs a;
     fill_image_args(a, g, grid, p, rays, n, w.perm, w.ckpt, w.nsteps);

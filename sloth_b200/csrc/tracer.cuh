@@ -1390,10 +1390,14 @@ inline int bucket_bits_for(long long n) {
 
 // Morton pre-pass of n rays into bucket order: keys, histogram (2^bbits
 // buckets, zeroed by the caller), exclusive scan, scatter into perm/skeys.
+// The buckets are the keys' top bbits bits; with fine_buckets, the top bbits
+// of the bits the grid's keys use, so that a small grid's transverse cells
+// get buckets of their own (for kernels that trace rays in bucket order
+// without a further sort).
 template <class R>
 inline int launch_prepass(const SlothGridDesc* g, int axis, const R* rays, long long n, int bbits,
                           unsigned* keys, unsigned* hist, unsigned* perm, unsigned* skeys, int sms,
-                          cudaStream_t s) {
+                          cudaStream_t s, bool fine_buckets = false) {
     const int t1 = axis == 0 ? 1 : 0;
     const int t2 = axis == 2 ? 1 : 2;
     KeyArgs ka;
@@ -1411,6 +1415,13 @@ inline int launch_prepass(const SlothGridDesc* g, int axis, const R* rays, long 
     ka.t1 = t1;
     ka.t2 = t2;
     ka.bucket_shift = 30 - bbits;
+    if (fine_buckets) {
+        int tb = 0;   // bits of the largest transverse cell coordinate
+        for (int t : {t1, t2})
+            while (((g->n[t] - 2) >> ka.shift[t]) >> tb) ++tb;
+        const int used = 2 * tb + 10;
+        ka.bucket_shift = used > bbits ? used - bbits : 0;
+    }
     ka.keys = keys;
     ka.hist = hist;
     const long long nblk = (n + 255) / 256;
@@ -1419,7 +1430,7 @@ inline int launch_prepass(const SlothGridDesc* g, int axis, const R* rays, long 
     note_launch();
     scan_kernel<<<1, 1024, 0, s>>>(hist, 1 << bbits);
     note_launch();
-    scatter_kernel<<<kb, 256, 0, s>>>(keys, n, 30 - bbits, hist, perm, skeys);
+    scatter_kernel<<<kb, 256, 0, s>>>(keys, n, ka.bucket_shift, hist, perm, skeys);
     note_launch();
     return cuda_status(cudaGetLastError());
 }
