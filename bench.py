@@ -80,6 +80,18 @@ def committed_lane_ops():
     return (float(m.group(1)) if m else None), (w.group(1).strip() if w else None)
 
 
+def committed_backward_lane_ops():
+    """FP32 lane-operations per ray-step of the adjoint backward kernel, from the
+    committed ncu instruction-mix summary of the detector-image workload."""
+    p = os.path.join(ROOT, "profiles", "adjoint_kernels_kolmogorov128_1e6.md")
+    if not os.path.exists(p):
+        return None, None
+    text = open(p).read()
+    m = re.search(r"backward_fp32_lane_ops_per_ray_step:\s*([0-9.eE+]+)", text)
+    w = re.search(r"backward_lane_ops_workload:\s*(.+)", text)
+    return (float(m.group(1)) if m else None), (w.group(1).strip() if w else None)
+
+
 def committed_traffic(args):
     """DRAM bytes per trace launch from the committed ncu summary of the
     512^3 / 1e7-ray workload (None for any other workload)."""
@@ -654,6 +666,17 @@ def run_sloth(args):
         pipe_peak = sms * 128 * sm_mhz * 1e6 / 1e12
         pipe_achieved = ray_steps * lane_ops / (kms / 1e3) / 1e12 if lane_ops else None
         gather_gbs = ray_steps * BYTES_PER_RAY_STEP / (kms / 1e3) / 1e9
+        if adj:
+            # the adjoint backward against the same FP32-pipe peak (its kernel is issue-bound; see
+            # the profile the lane-operation count comes from)
+            bl, bl_where = committed_backward_lane_ops()
+            if bl:
+                ach = adj["ray_steps"] * bl / (adj["backward_ms"] / 1e3) / 1e12
+                adj["backward_roofline"] = {"bound": "fp32_pipe", "achieved": ach, "peak": pipe_peak,
+                                            "unit": "T FP32 lane-ops/s", "frac": ach / pipe_peak,
+                                            "lane_ops_per_ray_step": bl, "lane_ops_from": bl_where,
+                                            "note": "backward_ms includes the loss gradient and the pack "
+                                                    "adjoint; the peak uses the trace's sampled SM clock"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
