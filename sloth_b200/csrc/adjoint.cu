@@ -36,6 +36,7 @@
 // stage's cell and added to the grid-gradient buffer when the cell changes.
 // pack_adjoint_kernel maps d L / d(packed grid) through the transposed
 // difference stencil of K1 to d L / d ne.
+#include <climits>
 #include <cmath>
 
 #include "tracer.cuh"
@@ -71,6 +72,7 @@ struct ImageArgs {
     const unsigned* perm;        // slot -> ray id (bucket order)
     double origin[3], w_of_v[3], inv_h[3];
     double S[3];                 // -(dtau/h)^2 / 2
+    float Sf[3];                 // S rounded to FP32 once on the host (the FP32 kernels' copy)
     int n_steps, ckpt_every, n_seg;
     int axis, t1, t2;
     double plane;                // detector plane (cells along axis)
@@ -85,6 +87,12 @@ struct ImageArgs {
     unsigned long long* total_steps;   // forward: steps of all rays are added here (may be null)
     const unsigned* accel_bound;       // float bits of max |S_k dq/du_k| over the grid (workspace)
 };
+
+// S_k in the kernel's precision: FP32 kernels read the host-rounded copy, so
+// no step converts it.
+template <class R> __device__ __forceinline__ R img_S(const ImageArgs& a, int k);
+template <> __device__ __forceinline__ float img_S<float>(const ImageArgs& a, int k) { return a.Sf[k]; }
+template <> __device__ __forceinline__ double img_S<double>(const ImageArgs& a, int k) { return a.S[k]; }
 
 // ---------------------------------------------------------------------------
 // Ray state and checkpoints.
@@ -273,13 +281,13 @@ __device__ __forceinline__ void accel(const ImageArgs& a, const typename P::R (&
         load_cell_f2(a, b, cc);
         const float2 fx = make_float2(f[0], f[0]), fy = make_float2(f[1], f[1]), fz = make_float2(f[2], f[2]);
         const float2 r0 = poly_eval2(cc.t[0], fx, fy, fz), r1 = poly_eval2(cc.t[1], fx, fy, fz);
-        A[0] = (R)a.S[0] * r0.y;
-        A[1] = (R)a.S[1] * r1.x;
-        A[2] = (R)a.S[2] * r1.y;
+        A[0] = img_S<R>(a, 0) * r0.y;
+        A[1] = img_S<R>(a, 1) * r1.x;
+        A[2] = img_S<R>(a, 2) * r1.y;
     } else {
         load_cell<P>(a, b, cc);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) A[k] = (R)a.S[k] * poly_eval<R>(cc.t[k], f[0], f[1], f[2]);
+        for (int k = 0; k < 3; ++k) A[k] = img_S<R>(a, k) * poly_eval<R>(cc.t[k], f[0], f[1], f[2]);
     }
 }
 
@@ -440,7 +448,7 @@ __device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const StageRec
     const float2 fx2 = make_float2(fx, fx), fy2 = make_float2(fy, fy), fz2 = make_float2(fz, fz);
     float gb[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) gb[k] = (float)a.S[k] * Abar[k];
+    for (int k = 0; k < 3; ++k) gb[k] = img_S<float>(a, k) * Abar[k];
     // J^T gb. Channel 1 (dq/du) is the .y half of pair 0, channels 2 and 3 are pair 1.
     const float2* t0 = cc.t[0];
     const float2* t1 = cc.t[1];
@@ -496,7 +504,7 @@ __device__ __forceinline__ void stage_adjoint(const ImageArgs& a, const StageRec
     const R fx = f[0], fy = f[1], fz = f[2];
     R gb[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) gb[k] = (R)a.S[k] * Abar[k];
+    for (int k = 0; k < 3; ++k) gb[k] = img_S<R>(a, k) * Abar[k];
     // J^T gb: derivatives of the three trilinear polynomials
     q[0] = q[1] = q[2] = R(0);
 #pragma unroll
@@ -646,6 +654,86 @@ __device__ __forceinline__ void splat(const ImageArgs& a, double pa, double pb) 
     }
 }
 
+// A CTA's splats, formed in shared memory and added to the image once per
+// pixel. The rays of a CTA share their entry cell, so their windows overlap
+// on the detector; adding each ray's taps to the image directly (17 x 17
+// reductions per ray at sigma = 2) made the image's L2 atomics a third of the
+// forward's time. Here the CTA takes the box of its rays' windows (clipped to
+// the image). When a window fits in the kSplatTile x kSplatTile tile at the
+// box's low corner, the ray's separable weights g(i - a) * norm (rows) and
+// g(j - b) (columns) over the tile go to shared memory, kSplatRays rays at a
+// time, and every thread sums ray products for four pixels of the tile:
+// pixel (r, c) = sum over rays of row_weight(r) * column_weight(c), a small
+// matrix product. Windows that do not fit are splatted directly. Every thread
+// of the CTA calls this (it synchronises the CTA).
+constexpr int kSplatTile = 32;     // pixels per side of a CTA's tile
+constexpr int kSplatRays = 64;     // rays staged per round
+constexpr int kSplatPitch = kSplatTile + 1;   // shared row pitch (conflict-free stores and loads)
+
+template <class P>
+__device__ __forceinline__ void splat_block(const ImageArgs& a, bool has, double pa, double pb) {
+    using R = typename P::R;
+    __shared__ R s_row[kSplatRays * kSplatPitch], s_col[kSplatRays * kSplatPitch];
+    __shared__ int s_box[2];
+    const int t = threadIdx.x;
+    int i0 = 0, j0 = 0, r0 = 0, r1 = -1, c0 = 0, c1 = -1;
+    if (has) {
+        i0 = (int)floor(pa - a.radius) + 1;
+        j0 = (int)floor(pb - a.radius) + 1;
+        r0 = max(i0, 0);
+        r1 = min(i0 + a.taps - 1, a.npx[0] - 1);
+        c0 = max(j0, 0);
+        c1 = min(j0 + a.taps - 1, a.npx[1] - 1);
+    }
+    const bool in = r0 <= r1 && c0 <= c1;
+    if (t == 0) s_box[0] = s_box[1] = INT_MAX;
+    __syncthreads();
+    if (in) {
+        atomicMin(&s_box[0], r0);
+        atomicMin(&s_box[1], c0);
+    }
+    __syncthreads();
+    const int br = s_box[0], bc = s_box[1];
+    const bool tiled = in && r1 < br + kSplatTile && c1 < bc + kSplatTile;
+    if (in && !tiled) splat<P>(a, pa, pb);
+    if (!__syncthreads_or(tiled)) return;
+    // this thread's four pixels: column c, rows r, r + 8, r + 16, r + 24
+    const int c = t & (kSplatTile - 1), rb = t >> 5;
+    static_assert(kAdjThreads == 256 && kSplatTile == 32, "four pixels per thread");
+    R acc[4] = {R(0), R(0), R(0), R(0)};
+    const R s = (R)a.sigma;
+    for (int base = 0; base < (int)blockDim.x; base += kSplatRays) {
+        if (t >= base && t < base + kSplatRays) {
+            R* rw = s_row + (t - base) * kSplatPitch;
+            R* cw = s_col + (t - base) * kSplatPitch;
+            for (int k = 0; k < kSplatTile; ++k) {
+                R g = R(0), dg;
+                const int ii = br + k;
+                if (tiled && ii >= r0 && ii <= r1) g = splat_g<R>((R)((double)ii - pa), s, dg) * (R)a.norm;
+                rw[k] = g;
+                R h = R(0);
+                const int jj = bc + k;
+                if (tiled && jj >= c0 && jj <= c1) h = splat_g<R>((R)((double)jj - pb), s, dg);
+                cw[k] = h;
+            }
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int u = 0; u < kSplatRays; ++u) {
+            const R h = s_col[u * kSplatPitch + c];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] += s_row[u * kSplatPitch + rb + 8 * q] * h;
+        }
+        __syncthreads();
+    }
+    R* img = reinterpret_cast<R*>(a.image);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int ii = br + rb + 8 * q, jj = bc + c;
+        if (acc[q] != R(0) && ii < a.npx[0] && jj < a.npx[1]) atomicAdd(img + (size_t)ii * a.npx[1] + jj, acc[q]);
+    }
+}
+
 // d L / d(pixel coordinates) from the image gradient.
 template <class P>
 __device__ __forceinline__ void splat_adjoint(const ImageArgs& a, double pa, double pb, double& ga, double& gb) {
@@ -777,6 +865,8 @@ __global__ void __launch_bounds__(kAdjThreads, adj_fwd_min_blocks<P>()) image_fo
     __syncthreads();
     const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int t = 0;
+    bool has = false;     // the ray meets the detector plane at (pa, pb) pixels
+    double pa = 0.0, pb = 0.0;
     if (slot < a.n) {
         const unsigned id = a.perm[slot];
         const R* rays = reinterpret_cast<const R*>(a.rays);
@@ -816,9 +906,10 @@ __global__ void __launch_bounds__(kAdjThreads, adj_fwd_min_blocks<P>()) image_fo
         }
         store_state<P>(a, a.n_seg, slot, r);
         a.nsteps[slot] = t;
-        double pa, pb, tt, p[3], w[3];
-        if (detector_point<P>(a, r, pa, pb, tt, p, w)) splat<P>(a, pa, pb);
+        double tt, p[3], w[3];
+        has = detector_point<P>(a, r, pa, pb, tt, p, w);
     }
+    splat_block<P>(a, has, pa, pb);
     block_add((unsigned long long)t, &s_steps, a.total_steps);
 }
 
@@ -1025,6 +1116,7 @@ static void fill_image_args(ImageArgs& a, const SlothGridDesc* g, const void* gr
         a.inv_h[k] = 1.0 / h;
         a.w_of_v[k] = (p->dtau / h) / kC;
         a.S[k] = -0.5 * (p->dtau / h) * (p->dtau / h);
+        a.Sf[k] = (float)a.S[k];
     }
     a.n_steps = p->n_steps;
     a.ckpt_every = p->ckpt_every;
