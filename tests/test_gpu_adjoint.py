@@ -84,6 +84,21 @@ def test_image_and_gradient_f32_match_oracle():
     assert float((g - g_o).norm() / g_o.norm()) < 1e-4
 
 
+@pytest.mark.parametrize("precision,tol", [("f64", 1e-11), ("f32", 2e-5)])
+def test_image_with_tiled_and_direct_splats(precision, tol):
+    # A CTA splats the rays whose windows fit a 32 x 32 pixel tile in shared
+    # memory and the others directly. On a 96 x 96 detector, 256 rays from
+    # about 50 entry cells spread their windows over more than one tile, so
+    # both paths run in the same CTAs; the image must equal the oracle's.
+    h, _, ne1, rays, spec = _small()
+    spec = adjoint.DetectorSpec(window=spec.window, plane=spec.plane, dtau=spec.dtau, n_px=(96, 96),
+                                sigma_px=spec.sigma_px, n_steps=spec.n_steps, ckpt_every=spec.ckpt_every)
+    img_o = _oracle(ne1, rays, h, spec).detach()
+    img, _ = _kernel(ne1, rays, h, spec, precision)
+    assert float(img.sum()) > 0.5 * rays.shape[1]
+    assert _rel(img, img_o) < tol
+
+
 def test_gradient_independent_of_checkpoint_length():
     h, ne0, ne1, rays, _ = _small()
     grads = []
