@@ -100,6 +100,8 @@ struct TraceArgs {
     double S[3];               // -(dtau/h)^2 / 2
     float Sf[3];               // the same, rounded to FP32 once here (the FP32 tracer reads these
                                // instead of converting the doubles inside its loop)
+    float S8f[3], S2f[3], S6f[3];   // Sf/8, Sf/2 and fl(1/6)*Sf in FP32: the paired RKN step's
+                                    // unit-step coefficients with S folded in
     float ope2f, cl_lof, cl_wf;
     float inv_ope2f;           // 1 / ope2 (q from x = ope2 * q)
     float accel_bound;         // bound on |acceleration| (cells per step^2), 0 when unknown
@@ -635,61 +637,86 @@ __device__ __forceinline__ void rkn_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
     auto mphi2 = [&](float2 x) { return UNIT ? x : __fmul2_rn(bc2(phi), x); };
     const float hphi = 0.5f * phi, phi6 = phi * (1.0f / 6.0f), phi2_6 = phi * phi6;
     const float phi2_8 = 0.125f * phi * phi, phi2_2 = 0.5f * phi * phi;
-    const float S0 = a.Sf[0];
-    const float2 S12 = make_float2(a.Sf[1], a.Sf[2]);
-    const float2 hphi2 = bc2(hphi), phi22 = bc2(phi), phi2_82 = bc2(phi2_8), phi2_22 = bc2(phi2_2);
+    // The accelerations enter the step only through the stage points and the
+    // two weighted sums, so S multiplies the step's coefficients rather than
+    // every stage's gradient: k8 = phi^2 S/8, k2 = phi^2 S/2 (stage points),
+    // k6 = phi^2 S/6 (position), kw = phi S/6 (velocity). Unit steps read them
+    // from the arguments, formed there exactly as here at phi = 1.
+    float k8x, k2x, k6x, kwx;
+    float2 k8yz, k2yz, k6yz, kwyz;
+    if constexpr (UNIT) {
+        k8x = a.S8f[0];
+        k2x = a.S2f[0];
+        k6x = kwx = a.S6f[0];
+        k8yz = make_float2(a.S8f[1], a.S8f[2]);
+        k2yz = make_float2(a.S2f[1], a.S2f[2]);
+        k6yz = kwyz = make_float2(a.S6f[1], a.S6f[2]);
+    } else {
+        const float S0 = a.Sf[0];
+        const float2 S12 = make_float2(a.Sf[1], a.Sf[2]);
+        k8x = __fmul_rn(phi2_8, S0);
+        k2x = __fmul_rn(phi2_2, S0);
+        k6x = __fmul_rn(phi2_6, S0);
+        kwx = __fmul_rn(phi6, S0);
+        k8yz = __fmul2_rn(bc2(phi2_8), S12);
+        k2yz = __fmul2_rn(bc2(phi2_2), S12);
+        k6yz = __fmul2_rn(bc2(phi2_6), S12);
+        kwyz = __fmul2_rn(bc2(phi6), S12);
+    }
+    const float2 hphi2 = bc2(hphi), phi22 = bc2(phi);
     // Every rounding is explicit (intrinsics), so that each kernel that
     // inlines this step (the tracer's and the server's) rounds alike.
     const float phx = r.p[0].s, plx = r.p[0].c, wex = r.w[0].s + r.w[0].c;
     const float2 phyz = make_float2(r.p[1].s, r.p[2].s), plyz = make_float2(r.p[1].c, r.p[2].c);
     const float2 weyz = __fadd2_rn(make_float2(r.w[1].s, r.w[2].s), make_float2(r.w[1].c, r.w[2].c));
     Sample<PolF32> s;
-    // stage 1 at p
+    // stage 1 at p; gA = g1 + 2 g2 and gW = g1 + 4 g2 + g3 are the gradient
+    // sums (S applied in the coefficients)
     sample_f2<IB, MODE>(a, phx, plx, phyz, plyz, s, cc);
     float g = s.n1;
     float kq = s.k;
-    float sAx = __fmul_rn(S0, s.g0);
-    float2 sAyz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
-    float sWx = sAx;
-    float2 sWyz = sAyz;
+    float gAx = s.g0;
+    float2 gAyz = make_float2(s.g1, s.g2);
+    float gWx = gAx;
+    float2 gWyz = gAyz;
     // stage 2 at p + phi*w/2 + phi^2 A1/8
-    float stx = __fadd_rn(plx, __fmaf_rn(phi2_8, sAx, __fmul_rn(hphi, wex)));
-    float2 styz = __fadd2_rn(plyz, __ffma2_rn(phi2_82, sAyz, __fmul2_rn(hphi2, weyz)));
+    float stx = __fadd_rn(plx, __fmaf_rn(k8x, gAx, __fmul_rn(hphi, wex)));
+    float2 styz = __fadd2_rn(plyz, __ffma2_rn(k8yz, gAyz, __fmul2_rn(hphi2, weyz)));
     sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
     {
-        const float Ax = __fmul_rn(S0, s.g0);
-        const float2 Ayz = __fmul2_rn(S12, make_float2(s.g1, s.g2));
-        sAx = __fmaf_rn(2.0f, Ax, sAx);
-        sAyz = __ffma2_rn(bc2(2.0f), Ayz, sAyz);
-        sWx = __fmaf_rn(4.0f, Ax, sWx);
-        sWyz = __ffma2_rn(bc2(4.0f), Ayz, sWyz);
+        const float Gx = s.g0;
+        const float2 Gyz = make_float2(s.g1, s.g2);
+        gAx = __fmaf_rn(2.0f, Gx, gAx);
+        gAyz = __ffma2_rn(bc2(2.0f), Gyz, gAyz);
+        gWx = __fmaf_rn(4.0f, Gx, gWx);
+        gWyz = __ffma2_rn(bc2(4.0f), Gyz, gWyz);
         // stage 3 at p + phi*w + phi^2 A2/2
-        stx = __fadd_rn(plx, __fmaf_rn(phi2_2, Ax, mphi(wex)));
-        styz = __fadd2_rn(plyz, __ffma2_rn(phi2_22, Ayz, mphi2(weyz)));
+        stx = __fadd_rn(plx, __fmaf_rn(k2x, Gx, mphi(wex)));
+        styz = __fadd2_rn(plyz, __ffma2_rn(k2yz, Gyz, mphi2(weyz)));
     }
     g = __fmaf_rn(4.0f, s.n1, g);
     kq = __fmaf_rn(4.0f, s.k, kq);
     sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
-    sWx = __fmaf_rn(S0, s.g0, sWx);
-    sWyz = __ffma2_rn(S12, make_float2(s.g1, s.g2), sWyz);
+    gWx = __fadd_rn(gWx, s.g0);
+    gWyz = __fadd2_rn(gWyz, make_float2(s.g1, s.g2));
     g = __fadd_rn(g, s.n1);
     kq = __fadd_rn(kq, s.k);
     // x: the scalar update
     if constexpr (UNIT)
-        r.p[0].add(__fadd_rn(r.w[0].hi(), __fadd_rn(r.w[0].lo(), __fmul_rn(phi2_6, sAx))));
+        r.p[0].add(__fadd_rn(r.w[0].hi(), __fadd_rn(r.w[0].lo(), __fmul_rn(k6x, gAx))));
     else
-        r.p[0].add(__fmaf_rn(phi, r.w[0].hi(), __fmaf_rn(phi, r.w[0].lo(), __fmul_rn(phi2_6, sAx))));
-    r.w[0].add(__fmul_rn(phi6, sWx));
+        r.p[0].add(__fmaf_rn(phi, r.w[0].hi(), __fmaf_rn(phi, r.w[0].lo(), __fmul_rn(k6x, gAx))));
+    r.w[0].add(__fmul_rn(kwx, gWx));
     // y, z: the same update on pairs
     {
         const float2 whi = make_float2(r.w[1].s, r.w[2].s), wlo = make_float2(r.w[1].c, r.w[2].c);
-        const float2 dp = UNIT ? __fadd2_rn(whi, __fadd2_rn(wlo, __fmul2_rn(bc2(phi2_6), sAyz)))
-                               : __ffma2_rn(phi22, whi, __ffma2_rn(phi22, wlo, __fmul2_rn(bc2(phi2_6), sAyz)));
+        const float2 dp = UNIT ? __fadd2_rn(whi, __fadd2_rn(wlo, __fmul2_rn(k6yz, gAyz)))
+                               : __ffma2_rn(phi22, whi, __ffma2_rn(phi22, wlo, __fmul2_rn(k6yz, gAyz)));
         float2 ps = phyz, pc = plyz;
         kahan2(ps, pc, dp);
         r.p[1].s = ps.x; r.p[2].s = ps.y; r.p[1].c = pc.x; r.p[2].c = pc.y;
         float2 ws = whi, wc = wlo;
-        kahan2(ws, wc, __fmul2_rn(bc2(phi6), sWyz));
+        kahan2(ws, wc, __fmul2_rn(kwyz, gWyz));
         r.w[1].s = ws.x; r.w[2].s = ws.y; r.w[1].c = wc.x; r.w[2].c = wc.y;
     }
     r.ph += (double)mphi(g);
@@ -1476,6 +1503,11 @@ inline void fill_trace_args(TraceArgs& ta, const SlothGridDesc* g, const void* g
         ta.v_of_w[k] = kC * h / p->dtau;
         ta.S[k] = -0.5 * (p->dtau / h) * (p->dtau / h);
         ta.Sf[k] = (float)ta.S[k];
+        // as the step forms them at phi = 1: exact scalings by 1/8 and 1/2, one
+        // FP32 rounding of fl(1/6) * Sf
+        ta.S8f[k] = 0.125f * ta.Sf[k];
+        ta.S2f[k] = 0.5f * ta.Sf[k];
+        ta.S6f[k] = (1.0f / 6.0f) * ta.Sf[k];
     }
     ta.phase_scale = (p->omega / kC) * p->dtau / 6.0;
     ta.tau_scale = p->kappa_q2 * p->dtau / 6.0;   // times cl_lo below for the sub-critical mode
