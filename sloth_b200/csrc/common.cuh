@@ -67,6 +67,13 @@ struct AccF {
         c = y - (t - s);
         s = t;
     }
+    // add(a * b) with the product's rounding folded into the compensated add
+    __device__ __forceinline__ void add_fma(float a, float b) {
+        const float y = __fmaf_rn(a, b, c);
+        const float t = s + y;
+        c = y - (t - s);
+        s = t;
+    }
     __device__ __forceinline__ float val() const { return s + c; }
     __device__ __forceinline__ double vald() const { return (double)s + (double)c; }
     __device__ __forceinline__ float hi() const { return s; }

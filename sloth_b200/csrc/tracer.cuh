@@ -100,7 +100,7 @@ struct TraceArgs {
     double S[3];               // -(dtau/h)^2 / 2
     float Sf[3];               // the same, rounded to FP32 once here (the FP32 tracer reads these
                                // instead of converting the doubles inside its loop)
-    float S8f[3], S2f[3], S6f[3];   // Sf/8, Sf/2 and fl(1/6)*Sf in FP32: the paired RKN step's
+    float S4f[3], S2f[3], S6f[3];   // Sf/4, Sf/2 and fl(1/6)*Sf in FP32: the paired RKN step's
                                     // unit-step coefficients with S folded in
     float ope2f, cl_lof, cl_wf;
     float inv_ope2f;           // 1 / ope2 (q from x = ope2 * q)
@@ -627,6 +627,14 @@ __device__ __forceinline__ void kahan2(float2& s, float2& c, float2 x) {
     s = t;
 }
 
+// kahan2 of a * b, the product's rounding folded into the compensated add
+__device__ __forceinline__ void kahan2_fma(float2& s, float2& c, float2 a, float2 b) {
+    const float2 y = __ffma2_rn(a, b, c);
+    const float2 t = __fadd2_rn(s, y);
+    c = __fadd2_rn(y, __ffma2_rn(s, bc2(1.0f), make_float2(-t.x, -t.y)) );
+    s = t;
+}
+
 // UNIT: phi is 1 (every step but a cut one); the multiplications by phi are
 // left out, which gives bitwise the results of the general form at phi = 1
 // (fma(1, a, b) rounds as a + b).
@@ -636,29 +644,30 @@ __device__ __forceinline__ void rkn_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
     auto mphi = [&](float x) { return UNIT ? x : __fmul_rn(phi, x); };
     auto mphi2 = [&](float2 x) { return UNIT ? x : __fmul2_rn(bc2(phi), x); };
     const float hphi = 0.5f * phi, phi6 = phi * (1.0f / 6.0f), phi2_6 = phi * phi6;
-    const float phi2_8 = 0.125f * phi * phi, phi2_2 = 0.5f * phi * phi;
+    const float phi2_2 = 0.5f * phi * phi;
     // The accelerations enter the step only through the stage points and the
     // two weighted sums, so S multiplies the step's coefficients rather than
-    // every stage's gradient: k8 = phi^2 S/8, k2 = phi^2 S/2 (stage points),
-    // k6 = phi^2 S/6 (position), kw = phi S/6 (velocity). Unit steps read them
-    // from the arguments, formed there exactly as here at phi = 1.
-    float k8x, k2x, k6x, kwx;
-    float2 k8yz, k2yz, k6yz, kwyz;
+    // every stage's gradient: k4 = phi S/4 and k2 = phi^2 S/2 (stage points,
+    // p + (phi/2)(w + k4 G1) and p + phi w + k2 G2), k6 = phi^2 S/6 (position),
+    // kw = phi S/6 (velocity). Unit steps read them from the arguments, formed
+    // there exactly as here at phi = 1.
+    float k4x, k2x, k6x, kwx;
+    float2 k4yz, k2yz, k6yz, kwyz;
     if constexpr (UNIT) {
-        k8x = a.S8f[0];
+        k4x = a.S4f[0];
         k2x = a.S2f[0];
         k6x = kwx = a.S6f[0];
-        k8yz = make_float2(a.S8f[1], a.S8f[2]);
+        k4yz = make_float2(a.S4f[1], a.S4f[2]);
         k2yz = make_float2(a.S2f[1], a.S2f[2]);
         k6yz = kwyz = make_float2(a.S6f[1], a.S6f[2]);
     } else {
         const float S0 = a.Sf[0];
         const float2 S12 = make_float2(a.Sf[1], a.Sf[2]);
-        k8x = __fmul_rn(phi2_8, S0);
+        k4x = __fmul_rn(0.25f * phi, S0);
         k2x = __fmul_rn(phi2_2, S0);
         k6x = __fmul_rn(phi2_6, S0);
         kwx = __fmul_rn(phi6, S0);
-        k8yz = __fmul2_rn(bc2(phi2_8), S12);
+        k4yz = __fmul2_rn(bc2(0.25f * phi), S12);
         k2yz = __fmul2_rn(bc2(phi2_2), S12);
         k6yz = __fmul2_rn(bc2(phi2_6), S12);
         kwyz = __fmul2_rn(bc2(phi6), S12);
@@ -679,9 +688,9 @@ __device__ __forceinline__ void rkn_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
     float2 gAyz = make_float2(s.g1, s.g2);
     float gWx = gAx;
     float2 gWyz = gAyz;
-    // stage 2 at p + phi*w/2 + phi^2 A1/8
-    float stx = __fadd_rn(plx, __fmaf_rn(k8x, gAx, __fmul_rn(hphi, wex)));
-    float2 styz = __fadd2_rn(plyz, __ffma2_rn(k8yz, gAyz, __fmul2_rn(hphi2, weyz)));
+    // stage 2 at p + phi*w/2 + phi^2 A1/8 = p + (phi/2)(w + k4 G1)
+    float stx = __fmaf_rn(hphi, __fmaf_rn(k4x, gAx, wex), plx);
+    float2 styz = __ffma2_rn(hphi2, __ffma2_rn(k4yz, gAyz, weyz), plyz);
     sample_f2<IB, MODE>(a, phx, stx, phyz, styz, s, cc);
     {
         const float Gx = s.g0;
@@ -703,20 +712,20 @@ __device__ __forceinline__ void rkn_step_f2(const TraceArgs& a, Ray<PolF32>& r, 
     kq = __fadd_rn(kq, s.k);
     // x: the scalar update
     if constexpr (UNIT)
-        r.p[0].add(__fadd_rn(r.w[0].hi(), __fadd_rn(r.w[0].lo(), __fmul_rn(k6x, gAx))));
+        r.p[0].add(__fadd_rn(r.w[0].hi(), __fmaf_rn(k6x, gAx, r.w[0].lo())));
     else
-        r.p[0].add(__fmaf_rn(phi, r.w[0].hi(), __fmaf_rn(phi, r.w[0].lo(), __fmul_rn(k6x, gAx))));
-    r.w[0].add(__fmul_rn(kwx, gWx));
+        r.p[0].add(__fmaf_rn(phi, r.w[0].hi(), __fmaf_rn(k6x, gAx, __fmul_rn(phi, r.w[0].lo()))));
+    r.w[0].add_fma(kwx, gWx);
     // y, z: the same update on pairs
     {
         const float2 whi = make_float2(r.w[1].s, r.w[2].s), wlo = make_float2(r.w[1].c, r.w[2].c);
-        const float2 dp = UNIT ? __fadd2_rn(whi, __fadd2_rn(wlo, __fmul2_rn(k6yz, gAyz)))
-                               : __ffma2_rn(phi22, whi, __ffma2_rn(phi22, wlo, __fmul2_rn(k6yz, gAyz)));
+        const float2 dp = UNIT ? __fadd2_rn(whi, __ffma2_rn(k6yz, gAyz, wlo))
+                               : __ffma2_rn(phi22, whi, __ffma2_rn(k6yz, gAyz, __fmul2_rn(phi22, wlo)));
         float2 ps = phyz, pc = plyz;
         kahan2(ps, pc, dp);
         r.p[1].s = ps.x; r.p[2].s = ps.y; r.p[1].c = pc.x; r.p[2].c = pc.y;
         float2 ws = whi, wc = wlo;
-        kahan2(ws, wc, __fmul2_rn(kwyz, gWyz));
+        kahan2_fma(ws, wc, kwyz, gWyz);
         r.w[1].s = ws.x; r.w[2].s = ws.y; r.w[1].c = wc.x; r.w[2].c = wc.y;
     }
     r.ph += (double)mphi(g);
@@ -1503,9 +1512,9 @@ inline void fill_trace_args(TraceArgs& ta, const SlothGridDesc* g, const void* g
         ta.v_of_w[k] = kC * h / p->dtau;
         ta.S[k] = -0.5 * (p->dtau / h) * (p->dtau / h);
         ta.Sf[k] = (float)ta.S[k];
-        // as the step forms them at phi = 1: exact scalings by 1/8 and 1/2, one
+        // as the step forms them at phi = 1: exact scalings by 1/4 and 1/2, one
         // FP32 rounding of fl(1/6) * Sf
-        ta.S8f[k] = 0.125f * ta.Sf[k];
+        ta.S4f[k] = 0.25f * ta.Sf[k];
         ta.S2f[k] = 0.5f * ta.Sf[k];
         ta.S6f[k] = (1.0f / 6.0f) * ta.Sf[k];
     }
