@@ -16,7 +16,8 @@
 // all admitted jobs (`quantum` tiles per job per round, up to
 // `tiles_per_step`) and launches the iteration: a captured CUDA graph that
 // copies the work list to the device and runs one persistent serving kernel
-// per tracer mode on parallel branches. Two iterations can be in flight on
+// per tracer mode on parallel branches (the inverse-bremsstrahlung path times
+// the interior fast path, each kernel with one copy of the step). Two iterations can be in flight on
 // two streams, so one iteration's tail overlaps the next one's start. Jobs
 // that arrive while others are running join at the next iteration and their
 // tiles run in the same kernels as the others' (continuous batching).
@@ -38,7 +39,10 @@
 
 namespace sloth {
 
-constexpr int kModes = 3;   // the inverse-bremsstrahlung paths IB_OFF, IB_SUBCRITICAL, IB_GENERAL
+// Tracer modes: the inverse-bremsstrahlung path (IB_OFF, IB_SUBCRITICAL,
+// IB_GENERAL) times the fast path (interior runs with interior sampling when
+// the job's density range allows them, none otherwise); mode = 2 * IB + fast.
+constexpr int kModes = 6;
 
 struct WorkItem {
     int slot;
@@ -52,7 +56,7 @@ struct WorkHeader {
     int pad;
 };
 
-template <int IB>
+template <int IB, int FAST>
 __global__ void __launch_bounds__(kThreads, SLOTH_TRACE_MIN_BLOCKS)
 serve_kernel(const TraceArgs* __restrict__ table, WorkHeader* hdr, const WorkItem* __restrict__ items, int mode) {
     __shared__ TraceArgs s_args;
@@ -94,11 +98,9 @@ serve_kernel(const TraceArgs* __restrict__ table, WorkHeader* hdr, const WorkIte
         const long long start = (long long)s_tile * kTile;
         const int cnt = (int)min((long long)kTile, s_args.n - start);
         unsigned long long my_steps = 0;
-        // the job's density range bounds its accelerations: the interior fast path
-        if (interior_sampling_ok(s_args))
-            trace_tile<PolF32, IB, 1>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
-        else
-            trace_tile<PolF32, IB, 0>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
+        // FAST: the job's density range bounds its accelerations (the host
+        // sorted its tiles by interior_sampling_ok)
+        trace_tile<PolF32, IB, FAST>(s_args, start, cnt, s_key, s_id, &s_head, cc, my_steps);
         block_add(my_steps, &s_steps, s_args.total_steps);
     }
 }
@@ -267,8 +269,8 @@ static size_t job_bytes(long long n, const SlothTraceParams* p, int* bbits_out, 
 }
 
 static int graph_build(ServerImpl* s, IterSlot& is, int blocks[kModes]) {
-    // captured once per iteration slot: work list H2D, then the three mode
-    // kernels on parallel branches joined back into the slot's stream
+    // captured once per iteration slot: work list H2D, then the mode kernels
+    // on parallel branches joined back into the slot's stream
     cudaStream_t side[kModes];
     cudaEvent_t fork = nullptr, join[kModes];
     for (int m = 0; m < kModes; ++m) {
@@ -286,9 +288,12 @@ static int graph_build(ServerImpl* s, IterSlot& is, int blocks[kModes]) {
         for (int m = 0; m < kModes; ++m) {
             cudaStreamWaitEvent(side[m], fork, 0);
             switch (m) {
-                case IB_OFF: serve_kernel<IB_OFF><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
-                case IB_SUBCRITICAL: serve_kernel<IB_SUBCRITICAL><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
-                default: serve_kernel<IB_GENERAL><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
+                case 2 * IB_OFF: serve_kernel<IB_OFF, 0><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
+                case 2 * IB_OFF + 1: serve_kernel<IB_OFF, 1><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
+                case 2 * IB_SUBCRITICAL: serve_kernel<IB_SUBCRITICAL, 0><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
+                case 2 * IB_SUBCRITICAL + 1: serve_kernel<IB_SUBCRITICAL, 1><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
+                case 2 * IB_GENERAL: serve_kernel<IB_GENERAL, 0><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
+                default: serve_kernel<IB_GENERAL, 1><<<blocks[m], kThreads, 0, side[m]>>>(s->d_table, is.d_buf, items, m); break;
             }
             cudaEventRecord(join[m], side[m]);
             cudaStreamWaitEvent(is.stream, join[m], 0);
@@ -305,10 +310,10 @@ static int graph_build(ServerImpl* s, IterSlot& is, int blocks[kModes]) {
     return cuda_status(e);
 }
 
-template <int IB>
+template <int IB, int FAST>
 static int resident_blocks(int sms) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, serve_kernel<IB>, kThreads, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, serve_kernel<IB, FAST>, kThreads, 0) != cudaSuccess ||
         b < 1)
         b = 1;
     return b * sms;
@@ -414,7 +419,7 @@ static int admit_one(ServerImpl* s, Job& j) {
     fill_trace_args(ta, &ge->desc, s->arena.ptr(ge->off), &j.p, rays, j.n, &j.out, perm, skeys);
     e = cudaMemcpyAsync(s->d_table + j.slot, &ta, sizeof(TraceArgs), cudaMemcpyHostToDevice, s->admit);
     if (e != cudaSuccess) return cuda_status(e);
-    j.mode = trace_mode(&j.p);
+    j.mode = 2 * trace_mode(&j.p) + (interior_sampling_ok(ta) ? 1 : 0);
     j.tiles_total = (int)((j.n + kTile - 1) / kTile);
     j.tiles_assigned = 0;
     j.state = JOB_ADMITTED;
@@ -625,9 +630,12 @@ int sloth_server_create(const SlothServerConfig* cfg, SlothServer** out) {
         (e = cudaEventCreate(&s->t0)) != cudaSuccess || (e = cudaEventRecord(s->t0, s->admit)) != cudaSuccess)
         return fail(sloth::cuda_status(e));
     for (int i = cfg->max_jobs - 1; i >= 0; --i) s->free_slots.push_back(i);
-    int blocks[sloth::kModes] = {sloth::resident_blocks<sloth::IB_OFF>(s->sms),
-                                 sloth::resident_blocks<sloth::IB_SUBCRITICAL>(s->sms),
-                                 sloth::resident_blocks<sloth::IB_GENERAL>(s->sms)};
+    int blocks[sloth::kModes] = {sloth::resident_blocks<sloth::IB_OFF, 0>(s->sms),
+                                 sloth::resident_blocks<sloth::IB_OFF, 1>(s->sms),
+                                 sloth::resident_blocks<sloth::IB_SUBCRITICAL, 0>(s->sms),
+                                 sloth::resident_blocks<sloth::IB_SUBCRITICAL, 1>(s->sms),
+                                 sloth::resident_blocks<sloth::IB_GENERAL, 0>(s->sms),
+                                 sloth::resident_blocks<sloth::IB_GENERAL, 1>(s->sms)};
     const size_t wbytes = sizeof(sloth::WorkHeader) + sizeof(sloth::WorkItem) * (size_t)cfg->tiles_per_step;
     for (auto& is : s->it) {
         if ((e = cudaStreamCreateWithFlags(&is.stream, cudaStreamNonBlocking)) != cudaSuccess ||

@@ -990,7 +990,7 @@ __device__ __forceinline__ int interior_run(const TraceArgs& a, const Ray<P>& r)
 // Whether a trace's interior steps may sample without the grid test: its
 // accelerations are bounded by kInteriorAccel (accel_bound carries 0.1% of
 // headroom over the bound).
-__device__ __forceinline__ bool interior_sampling_ok(const TraceArgs& a) {
+__host__ __device__ __forceinline__ bool interior_sampling_ok(const TraceArgs& a) {
     return a.accel_bound > 0.0f && a.accel_bound <= (float)(kInteriorAccel * 1.001);
 }
 
