@@ -55,10 +55,9 @@ constexpr int kAdjThreads = 256;
 constexpr int kAdjBwdThreads = 128;
 constexpr int kAdjStateWords = 5;
 // Two FP32 builds of the backward: four CTAs per SM (128 registers) when
-// four segment buffers fit an SM's shared memory (checkpoints at most every
-// 21 steps), three (150 registers) otherwise. FP64 runs one CTA per SM.
-constexpr int kAdjBwdSmemPerSm = 228 * 1024;   // shared memory per SM
-constexpr int kAdjBwdSmemPerCta = 1024;        // reserved by the system per CTA
+// four segment buffers fit an SM's shared memory (on B200, 228 KB per SM and
+// 1 KB reserved per CTA: checkpoints at most every 21 steps), three (152
+// registers) otherwise. FP64 runs one CTA per SM.
 // The FP32 forward fits three 256-thread CTAs per SM (80 registers) without spilling.
 template <class P> constexpr int adj_fwd_min_blocks() { return sizeof(typename P::R) == 4 ? 3 : 1; }
 constexpr int kMaxCkptEvery = 32;
@@ -1248,7 +1247,12 @@ static int image_backward_impl(const SlothGridDesc* g, const void* grid, const S
         return err;
     };
     if constexpr (sizeof(typename P::R) == 4) {
-        if (4 * (smem + kAdjBwdSmemPerCta) <= (size_t)kAdjBwdSmemPerSm)
+        int dev = 0, per_sm = 0, reserved = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+            (e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess ||
+            (e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess)
+            return cuda_status(e);
+        if (4 * (smem + (size_t)reserved) <= (size_t)per_sm)
             e = launch(image_backward_kernel<P, 4>);
         else
             e = launch(image_backward_kernel<P, 3>);
