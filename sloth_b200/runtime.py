@@ -310,16 +310,25 @@ def _lane_workspace(n: int, dev, lane: int) -> torch.Tensor:
     return t
 
 
-STREAM_CHUNK_RAYS = 1 << 22
+STREAM_CHUNK_RAYS = 1 << 24
 STREAM_END_RAYS = 1 << 19
 
 
 def _chunk_bounds(n: int, cs: int) -> list:
-    """Chunk boundaries of n rays for trace_to_host: about `cs` rays per
-    chunk, but the first and the last chunk hold only STREAM_END_RAYS (when
-    cs is larger), because the first chunk's copy in and the last chunk's
-    copy out are the only copies no trace hides. Chunks between the ends
-    differ in size by one ray at most."""
+    """Chunk boundaries of n rays for trace_to_host: at most `cs` rays per
+    chunk. Above 8 * STREAM_END_RAYS rays (8 * cs when cs is smaller) the
+    first and the last chunk hold only that many, because the first chunk's
+    copy in and the last chunk's copy out are the only copies no trace hides;
+    below it every chunk is alike. Chunks between the ends differ in size by
+    one ray at most.
+
+    Each chunk is one trace launch, and a launch costs more than its rays'
+    share (its ramp and the tail of its tile queue: at 512^3 with a 3 mm
+    waist beam, 3M rays trace at 114 ms per 1e7 rays against 102 ms in one
+    launch of 1e7). So the default takes chunks as large as the end chunks'
+    traces can hide the middle chunks' copies behind: 1e7 rays go through as
+    0.5M, 9M and 0.5M (118 ms for solve() with that beam against 126 ms as
+    0.5M, three of 3M and 0.5M)."""
     if n <= 0:
         return [0, 0]
 
@@ -330,7 +339,7 @@ def _chunk_bounds(n: int, cs: int) -> list:
         return [lo + i * q + min(i, r) for i in range(k + 1)]
 
     end = min(cs, STREAM_END_RAYS)
-    if n <= 2 * end + cs:
+    if n <= 8 * end:
         return split(0, n)
     return [0] + split(end, n - end) + [n]
 
